@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of the D2Q9 time step (LLALBM's perform_lbm loop body) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one lattice-Boltzmann time step of the whole lattice.  The default
+workload is the 4096 x 4096 random porous channel (BGK tau 0.8, Zou-He
+velocity inlet u = 0.02, Zou-He pressure outlet rho = 1, 30 % solid discs of
+radius 3..12): its 2.4 GB FP64 state is far larger than L2, so every step reads
+HBM and the roofline fraction is meaningful.  `value` is MLUPS of the plain
+FP64 drop-in path (lattice nodes x steps / device time), with the FP32- and
+FP16-shifted storage forms reported beside it.
+
+Multi-GPU runs (torchrun, one rank per GPU) advance an independent replica of
+the lattice on every GPU (no data-path collective); `value` sums all replicas
+and the time is the maximum over ranks.
+
+--impl reference times the reference's own OpenMP CPU path (LLALBM's
+perform_lbm compiled from its headers, oracle/_ref/ref_runner_fast) on the
+host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "latticeboltzmannmethod-fonnesu-grassi-guffanti_b200")
+sys.path.insert(0, os.path.join(PKG, "python"))
+
+import llb_workloads as W  # noqa: E402
+
+METRIC = "MLUPS (D2Q9 lattice updates per second, all nodes)"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+REF_FAST = os.path.join(ROOT, "oracle", "_ref", "ref_runner_fast")
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def workload(name: str) -> dict:
+    if name == "porous4096":
+        return dict(name=name, desc="random porous channel 4096x4096, 30% solid discs r 3..12, BGK tau 0.8, "
+                    "Zou-He velocity inlet u=0.02, Zou-He pressure outlet rho=1",
+                    types=lambda: W.porous_types(4096, 4096), collision=0, tau=0.8, tau_even=0.8, tau_odd=0.8,
+                    inlet=("const", 0.02, 0.0), outlet_bc=2, rho_out=1.0, ref_args=[
+                        "--collision", "bgk", "--tau", "0.8", "--inlet", "zh", "--outlet", "zhp",
+                        "--inlet-u", "const:0.02:0", "--outlet-u", "pressure"])
+    if name == "cylinder1024x256":
+        te = 3.0 * (0.05 * 40 / 200) + 0.5
+        to = 0.25 * (1.0 / (te - 0.5)) + 0.5
+        return dict(name=name, desc="cylinder vortex street 1024x256, r=20 at (200,131), TRT magic 1/4, "
+                    "parabolic Zou-He inlet u_max=0.05, Zou-He pressure outlet rho=1",
+                    types=lambda: W.cylinder_types(), collision=1, tau=te, tau_even=te, tau_odd=to,
+                    inlet=("parabolic", 0.05, 1, 254), outlet_bc=2, rho_out=1.0, ref_args=[
+                        "--collision", "trt", "--tau-even", repr(te), "--magic", "0.25", "--inlet", "zh",
+                        "--outlet", "zhp", "--inlet-u", "parabolic:0.05:1:254", "--outlet-u", "pressure"])
+    if name == "cavity129":
+        return dict(name=name, desc="lid-driven cavity 129x129, BGK tau 0.884, lid u=(0.1,0)",
+                    types=lambda: W.cavity_types(129), collision=0, tau=0.884, tau_even=0.884, tau_odd=0.884,
+                    inlet=("const", 0.1, 0.0), outlet_bc=0, rho_out=1.0, ref_args=[
+                        "--collision", "bgk", "--tau", "0.884", "--inlet", "zh", "--outlet", "zh",
+                        "--inlet-u", "const:0.1:0"])
+    raise SystemExit(f"unknown workload {name}")
+
+
+def open_table(wl: dict, nodes: dict) -> np.ndarray:
+    ni, no = len(nodes["inlet"]), len(nodes["outlet"])
+    tab = np.zeros((1, ni + no, 2))
+    kind = wl["inlet"][0]
+    if kind == "const":
+        tab[0, :ni] = wl["inlet"][1:3]
+    else:
+        umax, i0, i1 = wl["inlet"][1:]
+        tab[0, :ni, 0] = [W.parabolic_u(int(i), umax, i0, i1) for i in nodes["inlet"][:, 0]]
+    if wl["outlet_bc"] == 2:
+        tab[0, ni:] = (wl["rho_out"], 0.0)
+    return tab
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int, period_ms: int = 50):
+        self.samples = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(index), "-lms", str(period_ms)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0: float, t1: float) -> dict:
+        inside = [s for t, s in self.samples if t0 <= t <= t1]
+        window = "timed"
+        if len(inside) < 3:
+            inside = [s for _, s in self.samples]
+            window = "run (timed region shorter than the sampling period)"
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(s[1]) for s in inside if num(s[1]) is not None]
+        mx = [num(s[2]) for s in inside if num(s[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for s in inside for n, v in zip(names, s[5:9]) if v.strip().lower() == "active"})
+        pw = [num(s[3]) for s in inside if num(s[3]) is not None]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(inside), "window": window,
+                "power_w_max": max(pw) if pw else None}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            from datetime import timedelta
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+            self.pg = dist
+            self.torch = torch
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU arms
+# ---------------------------------------------------------------------------
+def reference_cpu(wl: dict, types: np.ndarray, warmup: int, steps: int) -> dict:
+    """The reference's perform_lbm (OpenMP policies, all host threads) on the
+    same lattice: oracle/_ref/ref_runner_fast fed through Lattice::reinit."""
+    if not os.path.exists(REF_FAST):
+        return None
+    R, C = types.shape
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        raw = os.path.join(d, "types.u8")
+        np.ascontiguousarray(types.T).tofile(raw)  # column-major grid
+        cmd = [REF_FAST, "--types-raw", raw, str(R), str(C), "--policy", "omp", "--threads", str(threads),
+               *wl["ref_args"], "--timing", "--warmup", str(warmup), "--steps", str(steps), "--out", d]
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        p = subprocess.run(cmd, capture_output=True, text=True, cwd=d, env=env, timeout=1800)
+        if p.returncode != 0:
+            return {"error": p.stderr[-500:]}
+        line = [ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1]
+        r = json.loads(line)
+    mlups = R * C * steps / r["seconds"] / 1e6
+    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "reference",
+            "sample": f"LLALBM perform_lbm, OMPPolicy (OMPBGK/TRT, OMPBounceBack, OMPZouHe + Zou-He pressure "
+                      f"policy), {R}x{C} lattice, {steps} timed steps after {warmup} warm-up, "
+                      f"g++ -O3 -march=x86-64-v3 -fopenmp, {threads} threads",
+            "seconds": r["seconds"], "steps": steps}
+
+
+def oracle_cpu(wl: dict, types: np.ndarray, steps: int) -> dict:
+    """Fallback when the reference could not be compiled: the C restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import harness as H  # test infrastructure, used here only as the CPU baseline
+
+    lists = H.classify(types)
+    p = H.Params(collision=wl["collision"], tau=wl["tau"], tau_even=wl["tau_even"], tau_odd=wl["tau_odd"],
+                 outlet_bc=wl["outlet_bc"], rho_out=wl["rho_out"])
+    ins = "const:%r:0" % wl["inlet"][1] if wl["inlet"][0] == "const" else "parabolic:%r:%d:%d" % wl["inlet"][1:]
+    table = H.open_values(lists, ins, "pressure" if wl["outlet_bc"] == 2 else "const:0:0", 1)
+    t0 = time.perf_counter()
+    H.run_oracle(lists, p, steps, table)
+    s = time.perf_counter() - t0
+    R, C = types.shape
+    return {"value": R * C * steps / s / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
+            "sample": f"C restatement of the reference step, {R}x{C}, {steps} steps (incl. setup), 1 thread"}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def bytes_per_step(storage_bytes: int, n_active: int, n_nodes: int) -> int:
+    """Algorithmic HBM bytes of one step: 9 populations read and 9 written per
+    active node, plus the 1-byte node mask of every node."""
+    return 18 * storage_bytes * n_active + n_nodes
+
+
+def make_lattice(L, wl, nodes, R, C, storage, device):
+    g = L.CudaLattice(R, C, nodes["fluid"], nodes["wall"], nodes["inlet"], nodes["inlet_side"], nodes["outlet"],
+                      nodes["outlet_side"], nodes["obstacle"], nodes["obstacle_dirs"], collision=wl["collision"],
+                      tau=wl["tau"], tau_even=wl["tau_even"], tau_odd=wl["tau_odd"], outlet_bc=wl["outlet_bc"],
+                      storage=storage, device=device)
+    g.set_open_values(open_table(wl, nodes))
+    return g
+
+
+def time_form(L, wl, nodes, R, C, storage, device, warmup, steps, dist, sampler=None):
+    g = make_lattice(L, wl, nodes, R, C, storage, device)
+    g.init()
+    g.step(warmup)
+    g.synchronize()
+    dist.barrier()
+    g.synchronize()
+    t0 = time.perf_counter()
+    g.record(0)
+    g.step(steps)
+    g.record(1)
+    g.synchronize()
+    t1 = time.perf_counter()
+    dist.barrier()
+    ms = dist.max(g.elapsed_ms(0, 1))
+    g.check_numerics()
+    g.step(1, macro=True)
+    rho, u = g.macro()
+    return g, ms, (t0, t1), u
+
+
+def run_ours(a, dist):
+    import llalbm_cuda as L
+
+    wl = workload(a.workload)
+    types = wl["types"]()
+    R, C = types.shape
+    nodes = L.classify(types)
+    n_active = len(nodes["fluid"]) + len(nodes["inlet"]) + len(nodes["outlet"])
+    dev = dist.local
+    sampler = ClockSampler(dev)
+    forms = {}
+    u_ref = None
+    head = None
+    for storage, name, sb in ((0, "f64", 8), (1, "f32s", 4), (2, "f16s", 2)):
+        g, ms, (t0, t1), u = time_form(L, wl, nodes, R, C, storage, dev, a.warmup, a.steps, dist)
+        per = ms / a.steps
+        bps = bytes_per_step(sb, n_active, R * C)
+        form = {"mlups": dist.world * R * C / per / 1e3, "ms_per_step": per, "gb_s": bps / per / 1e6,
+                "bytes_per_step": bps}
+        if storage == 0:
+            u_ref = u
+            head = (g, ms, t0, t1)
+        else:
+            act = np.zeros((C, R), dtype=bool)
+            for k in ("fluid", "inlet", "outlet"):
+                act[nodes[k][:, 1], nodes[k][:, 0]] = True
+            diff = u[:, act] - u_ref[:, act]
+            form["u_rel_l2_vs_f64"] = float(np.sqrt((diff ** 2).sum() / (u_ref[:, act] ** 2).sum()))
+            g.close()
+        forms[name] = form
+    g, ms, t0, t1 = head
+    clocks = sampler.summary(t0, t1)
+
+    # end to end through the C ABI with host buffers: every step copies its
+    # boundary values from pinned host memory and reads back the step's
+    # stability flag (the reference's per-step LLALBM_DEBUG NaN scan).
+    try:
+        import torch
+        pinned = torch.empty((1, g.n_open, 2), dtype=torch.float64, pin_memory=True).numpy()
+    except Exception:
+        pinned = np.empty((1, g.n_open, 2))
+    pinned[...] = open_table(wl, nodes)
+    e2e_steps = max(1, min(a.steps, 200))
+    for _ in range(3):
+        g.set_open_values(pinned, g.t)
+        g.step(1)
+        g.check_numerics()
+    dist.barrier()
+    t_e = time.perf_counter()
+    for _ in range(e2e_steps):
+        g.set_open_values(pinned, g.t)
+        g.step(1)
+        g.check_numerics()
+    e_s = dist.max(time.perf_counter() - t_e)
+    g.close()
+    sampler.stop()
+
+    f64 = forms["f64"]
+    peaks = {}
+    if os.path.exists(PEAKS_FILE):
+        peaks = json.load(open(PEAKS_FILE))
+    peak = peaks.get("hbm_gbs") or FALLBACK_HBM_GBS
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get(f"{wl['name']}_f64_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": round(f64["mlups"], 1), "unit": "MLUPS", "n_gpus": dist.world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(f64["ms_per_step"], 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["name"], "description": wl["desc"], "rows": R, "cols": C,
+                   "active_nodes": n_active, "storage": "f64", "pattern": "AB (ping-pong)",
+                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
+                   "l2": "resident state 2 x 9 x 8 B x nodes, far larger than L2: no flush needed"
+                   if R * C >= 1 << 20 else "L2-resident lattice"},
+        "roofline": {"bound": "hbm", "achieved": round(f64["gb_s"], 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(f64["gb_s"] / peak, 4), "traffic": traffic,
+                     "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                     "algorithmic_bytes_per_launch": f64["bytes_per_step"]},
+        "forms": {k: {kk: (round(vv, 6) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                  for k, v in forms.items()},
+        "e2e": {"value": round(dist.world * R * C * e2e_steps / e_s / 1e6, 1), "unit": "MLUPS",
+                "h2d_bytes_per_step": int(pinned.nbytes), "d2h_bytes_per_step": 4, "steps": e2e_steps,
+                "path": "C ABI per step: llb_set_open_values (pinned host) + llb_step + llb_check_numerics"},
+        "gpu_launches": a.steps,
+        "clocks": clocks,
+    }
+    return line, wl, types
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="porous4096", choices=("porous4096", "cylinder1024x256", "cavity129"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+
+    if a.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        wl = workload(a.workload)
+        types = wl["types"]()
+        w, k = min(a.warmup, 2), max(1, min(a.steps, 5 if a.workload == "porous4096" else 200))
+        r = reference_cpu(wl, types, w, k)
+        if r is None:
+            r = oracle_cpu(wl, types, k)
+        if "error" in r:
+            print(json.dumps({"impl": "reference", "unavailable": "reference runner failed: " + r["error"][-200:]}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": round(r["value"], 3), "unit": "MLUPS",
+            "n_gpus": 0, "steps": k, "warmup": w, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "description": wl["desc"]},
+            "cpu_baseline": r, "e2e": {"value": round(r["value"], 3), "unit": "MLUPS",
+                                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return
+
+    dist = Dist(a.gpus)
+    line, wl, types = run_ours(a, dist)
+    if dist.rank == 0:
+        if dist.world == 1 and not a.no_cpu_baseline:
+            cb = reference_cpu(wl, types, 1, 3 if a.workload == "porous4096" else 100)
+            if cb is None or "error" in cb:
+                cb = oracle_cpu(wl, types, 2 if a.workload == "porous4096" else 100)
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

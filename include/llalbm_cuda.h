@@ -1,0 +1,198 @@
+/*
+ * llalbm_cuda.h -- C ABI of libllalbm_cuda.so, the sm_100a (B200) engine behind
+ * LLALBM's CUDA parallelization policy.
+ *
+ * The reference library's plugin boundary is the static interface of a
+ * ParallelizationPolicy (llalbm/src/core/parallelization/OMPPolicy.hpp:35-164),
+ * called by Lattice<P>::perform_lbm (llalbm/src/core/lattices/Lattice.hpp:288-438)
+ * once per policy function per step.  This engine fuses one whole step into one
+ * kernel, so its entry points replace groups of those policy calls; each
+ * declaration below names the calls it replaces.  Paths are relative to the
+ * LLALBM project root.
+ *
+ * Conventions: plain C types only; every function returns LLB_OK (0) or a
+ * negative LLB_E_* status and never throws; a handle is owned by one host
+ * thread at a time; distinct handles are independent (own CUDA stream and
+ * device buffers) and may be driven from distinct threads; the library owns
+ * every device buffer and the caller owns every host buffer.  Arrays follow
+ * the reference's Eigen tensor layouts (column-major, row index i fastest):
+ *   populations (R, C, 9) -> [i + R*(j + C*k)],  u (R, C, 2),  rho (R, C),
+ * and node coordinates are (i, j) pairs of int64, as Eigen::Index in
+ * Point / BoundaryPoint / ObstaclePoint (llalbm/src/utils/aliases.hpp:55-357).
+ */
+#ifndef LLALBM_CUDA_H
+#define LLALBM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LLB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define LLB_OK 0
+#define LLB_E_INVALID (-1)     /* bad argument (null pointer, bad enum, bad size) */
+#define LLB_E_GEOMETRY (-2)    /* node lists inconsistent (overlap, out of range, fluid on edge) */
+#define LLB_E_NOMEM (-3)       /* device or host allocation failed */
+#define LLB_E_CUDA (-4)        /* CUDA runtime error (message in llb_last_error) */
+#define LLB_E_NODEVICE (-5)    /* no usable CUDA device */
+#define LLB_E_STATE (-6)       /* call out of order (e.g. llb_step before llb_init) */
+#define LLB_E_NUMERIC (-7)     /* non-finite density detected on the device */
+#define LLB_E_UNSUPPORTED (-8) /* valid input outside what the engine implements */
+#define LLB_E_TIMEOUT (-9)     /* a bounded wait gave up */
+
+/* ---- enums ------------------------------------------------------------- */
+/* collision operators: BGKCollisionPolicy (collisions/BGKCollision.hpp:62-306),
+   TRTCollisionPolicy (collisions/TRTCollision.hpp:65-345) */
+#define LLB_BGK 0
+#define LLB_TRT 1
+/* population storage: FP64; FP32 or FP16 storing f_k - w_k (collision in FP32) */
+#define LLB_STORE_F64 0
+#define LLB_STORE_F32S 1
+#define LLB_STORE_F16S 2
+/* memory pattern: two buffers (ping-pong) or one buffer updated in place (A-A) */
+#define LLB_PATTERN_AB 0
+#define LLB_PATTERN_AA 1
+/* open-boundary policies: ZouHePolicy (boundaries/ZouHePolicy.hpp:58-123),
+   OpenBoundaryPolicy (boundaries/OpenBoundaryPolicy.hpp:58-61), and the Zou-He
+   pressure policy this project adds (llalbm_cuda/ZouHePressurePolicy.hpp) */
+#define LLB_BC_ZH_VELOCITY 0
+#define LLB_BC_OPEN 1
+#define LLB_BC_ZH_PRESSURE 2
+/* InputNodeType codes of the lattice file format (aliases.hpp:41-48) */
+#define LLB_NODE_FLUID 0
+#define LLB_NODE_SOLID 1
+#define LLB_NODE_BOUNDARY 2
+#define LLB_NODE_INLET 3
+#define LLB_NODE_OUTLET 4
+#define LLB_NODE_OBSTACLE 5
+/* llb_step flags */
+#define LLB_STEP_MACRO 1u /* write rho/u of the last step (Lattice.hpp:370-374 save) */
+
+/* ---- lattice description ----------------------------------------------- */
+typedef struct llb_lattice* llb_handle;
+
+/* Everything Lattice::reinit receives (Lattice.hpp:453-481) plus the policy
+   parameters the reference keeps in static members.  Side codes are the
+   reference's btypes (aliases.hpp:28-38); corner types mean "no closure". */
+typedef struct {
+    int64_t rows, cols;                                   /* lattice_dimensions */
+    int64_t n_fluid;    const int64_t* fluid_ij;          /* fluid_nodes */
+    int64_t n_wall;     const int64_t* wall_ij;           /* boundary_coord */
+    int64_t n_inlet;    const int64_t* inlet_ij;   const int32_t* inlet_side;   /* inlet_nodes_coord */
+    int64_t n_outlet;   const int64_t* outlet_ij;  const int32_t* outlet_side;  /* outlet_nodes_coord */
+    int64_t n_obstacle; const int64_t* obstacle_ij; const uint16_t* obstacle_dirs; /* may be NULL */
+    int32_t inlet_bc, outlet_bc;                          /* LLB_BC_* */
+    int32_t collision;                                    /* LLB_BGK / LLB_TRT */
+    double tau;                                           /* BGK: BGKCollisionPolicy<2>::tau */
+    double tau_even, tau_odd;                             /* TRT: TRTCollisionPolicy<2>::tau_even/odd */
+    int32_t storage;                                      /* LLB_STORE_* */
+    int32_t pattern;                                      /* LLB_PATTERN_* */
+    int32_t device;                                       /* CUDA ordinal */
+    int32_t open_table_rows;  /* per-step open-value ring capacity; 1 = values constant in time */
+} llb_desc;
+
+/* Node vectors as the reference builds them from a grid of InputNodeType codes. */
+typedef struct {
+    int64_t n_fluid, n_wall, n_inlet, n_outlet, n_obstacle;
+    int64_t* fluid_ij;
+    int64_t* wall_ij;
+    int64_t* inlet_ij;   int32_t* inlet_side;
+    int64_t* outlet_ij;  int32_t* outlet_side;
+    int64_t* obstacle_ij; uint16_t* obstacle_dirs;
+} llb_node_lists;
+
+/* ---- host-side lattice construction (no GPU needed) --------------------- */
+
+/* Replaces the classification of read_lattice_file (utils/readers/LatticeReader.hpp:488-519):
+   TensorLoopAccessor's row-major vector fill, verify_lattice_bounds,
+   identify_node_type (utils/analysis/NodeIdentification.hpp:45-110),
+   identify_obstacle_propagation (:137-211) and eliminate_non_wet_nodes (:229-242),
+   in O(R*C) instead of the reference's O(N^2) std::find scans.
+   `types` is (R, C) column-major InputNodeType codes.  counts[5] receives
+   fluid, wall, inlet, outlet and wet-obstacle counts. */
+int llb_classify_count(int64_t rows, int64_t cols, const uint8_t* types, int64_t counts[5]);
+/* Fills caller-allocated arrays sized by llb_classify_count (n_* fields are
+   checked against the counts). */
+int llb_classify_fill(int64_t rows, int64_t cols, const uint8_t* types, llb_node_lists* out);
+
+/* ---- lattice lifetime --------------------------------------------------- */
+
+/* Replaces Lattice::reinit / the Lattice constructors' tensor allocation
+   (Lattice.hpp:115-147, 173-239, 453-481) and the policy attach_nodes call
+   (OMPPolicy.hpp:127-131): validates the node lists, builds the 1-byte node
+   mask and uploads it, allocates the resident population buffers. */
+int llb_create(const llb_desc* desc, llb_handle* out);
+int llb_destroy(llb_handle h);
+
+/* Replaces InitializationPolicy::update_nodes (OMPPolicy.hpp:139-143,
+   initializers/InletOutletInitializer.hpp:90-129): values of the update
+   functions for steps t_first .. t_first+count-1, laid out
+   [count][n_inlet + n_outlet][2], inlets first.  Velocity and open nodes take
+   (u_x, u_y); Zou-He pressure nodes take (rho0, tangential u). */
+int llb_set_open_values(llb_handle h, int64_t t_first, int32_t count, const double* values);
+
+/* Replaces the initial equilibrium (Lattice.hpp:295-296, 326-328) and the
+   collision of step 0: afterwards the resident state is the post-collision
+   populations of step 0. */
+int llb_init(llb_handle h, uint32_t flags);
+
+/* Replaces `nsteps` iterations of the perform_lbm loop body (Lattice.hpp:338-410):
+   update_nodes, update_macro, calc_equilibrium, collide (+ open collide), stream
+   (+ open stream), wall and obstacle bounce-back, inlet and outlet closures --
+   one fused kernel per step.  LLB_STEP_MACRO keeps rho/u of the last step. */
+int llb_step(llb_handle h, int32_t nsteps, uint32_t flags);
+
+/* Index of the next step (number of collisions done). */
+int llb_get_step(llb_handle h, int64_t* step);
+
+/* ---- results (device -> host) ------------------------------------------ */
+
+/* global_rho / global_u of the last LLB_STEP_MACRO step (Lattice.hpp:58-70 getters
+   :499-506); either pointer may be NULL. */
+int llb_get_macro(llb_handle h, double* rho, double* u);
+/* `populations` (Lattice.hpp:492): streams the resident post-collision state
+   and applies bounce-back and the closures into an (R, C, 9) tensor.  Values
+   are defined for fluid, inlet and outlet nodes; other nodes read 0. */
+int llb_get_populations(llb_handle h, double* populations);
+/* `after_collision_populations` of the last step, (R, C, 9); 0 off active nodes. */
+int llb_get_post_collision(llb_handle h, double* populations);
+
+/* FlowAnalyzer<2>::compute_flow_properties (utils/analysis/FlowAnalyzer.hpp:348-451)
+   over the resident post-collision state: per-point terms exactly as the
+   reference, totals summed on the device with compensated FP64.
+   llb_set_force_points uploads the considered points once. */
+int llb_set_force_points(llb_handle h, const int64_t* ij, const uint16_t* dirs, int64_t n);
+int llb_flow_forces(llb_handle h, double lift_drag[2]);
+/* Gathers, for each considered point and each set direction bit, the
+   post-collision value the reference reads (FlowAnalyzer.hpp:394-427) into
+   values[n][8] (0 where the bit is clear), for feeding the reference analyzer. */
+int llb_gather_force_inputs(llb_handle h, double* values);
+
+/* Mass and momentum of the resident post-collision state (sum over fluid,
+   inlet and outlet nodes of sum_k f, c_x f, c_y f) with compensated FP64;
+   out[0] = mass, out[1] = momentum along j (u_x), out[2] = along -i (u_y). */
+int llb_mass_momentum(llb_handle h, double out[3]);
+
+/* ---- synchronisation, timing, errors ------------------------------------ */
+
+int llb_synchronize(llb_handle h);
+/* LLB_E_NUMERIC if any step since the last call produced a non-finite density
+   (the reference's LLALBM_DEBUG NaN scan, Lattice.hpp:412-422); clears the flag. */
+int llb_check_numerics(llb_handle h);
+/* CUDA events on the handle's stream: slot in [0, 8). */
+int llb_event_record(llb_handle h, int32_t slot);
+int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, float* ms);
+/* Device bytes held by the handle. */
+int llb_device_bytes(llb_handle h, int64_t* bytes);
+/* Message for the last error on this handle (or the last global error for NULL). */
+const char* llb_last_error(llb_handle h);
+int llb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LLALBM_CUDA_H */

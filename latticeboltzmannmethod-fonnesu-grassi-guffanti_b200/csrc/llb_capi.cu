@@ -1,0 +1,600 @@
+// C ABI of libllalbm_cuda.so (declared in include/llalbm_cuda.h).
+//
+// A handle owns one lattice on one device: its CUDA stream, the node mask, the
+// resident populations (two buffers, ping-pong), the open-boundary value ring,
+// output buffers and a device step counter.  Multi-step calls are replayed from
+// CUDA graphs of GRAPH_STEPS kernels (one graph per buffer parity).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/llalbm_cuda.h"
+#include "llb_launch.h"
+
+using namespace llb;
+
+namespace {
+
+constexpr int GRAPH_STEPS = 32;  // even: a replay returns the state to the same buffer
+thread_local std::string g_last_error;
+
+}  // namespace
+
+struct llb_lattice {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int storage = LLB_STORE_F64, pattern = LLB_PATTERN_AB;
+    int64_t R = 0, C = 0;
+    int ld = 0;
+    long long plane = 0;
+    size_t elem = 8;
+    void* f[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint8_t* d_mask = nullptr;
+    int32_t* d_open_idx = nullptr;
+    double2* d_open = nullptr;
+    int n_open = 0, cap = 1;
+    double* d_rho = nullptr;
+    double* d_u = nullptr;
+    double* d_dense = nullptr;
+    long long* d_step = nullptr;
+    unsigned* d_done = nullptr;
+    unsigned* d_flags = nullptr;
+    double2* d_partials = nullptr;
+    int partial_blocks = 0;
+    double* d_red = nullptr;
+    int64_t* d_fpts = nullptr;
+    uint16_t* d_fdirs = nullptr;
+    int64_t n_fpts = 0;
+    double* d_gather = nullptr;
+    Collision coll{};
+    int64_t step = 0;
+    bool initialized = false;
+    bool macro_valid = false;
+    cudaEvent_t ev[8] = {};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t bytes = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(llb_handle h, int code, const std::string& msg) {
+    g_last_error = msg;
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(llb_handle h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(h, e == cudaErrorMemoryAllocation ? LLB_E_NOMEM : LLB_E_CUDA, m);
+}
+
+#define LLB_CUDA(h, call)                                   \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+template <typename T>
+int dev_alloc(llb_handle h, T** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+    h->bytes += static_cast<int64_t>(bytes);
+    return LLB_OK;
+}
+
+int select_device(llb_handle h) {
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+    return LLB_OK;
+}
+
+LaunchCtx make_ctx(llb_handle h) {
+    LaunchCtx x{};
+    x.g.rows = static_cast<int>(h->R);
+    x.g.cols = static_cast<int>(h->C);
+    x.g.ld = h->ld;
+    x.g.plane = h->plane;
+    x.g.mask = h->d_mask;
+    x.g.open_idx = h->d_open_idx;
+    x.ot.vals = h->d_open;
+    x.ot.n_open = h->n_open;
+    x.ot.cap = h->cap;
+    x.c = h->coll;
+    x.mo.rho = h->d_rho;
+    x.mo.u = h->d_u;
+    x.ss.step = h->d_step;
+    x.ss.done = h->d_done;
+    x.ss.flags = h->d_flags;
+    x.stream = h->stream;
+    return x;
+}
+
+void release(llb_handle h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& g : h->graph)
+        if (g) cudaGraphExecDestroy(g);
+    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
+                    h->d_step, h->d_done, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+// ---------------------------------------------------------------------------
+// node mask
+// ---------------------------------------------------------------------------
+constexpr uint8_t UNSET = 0xff;
+
+int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vector<int32_t>& open_idx,
+               std::string& why) {
+    const int64_t R = d->rows, C = d->cols;
+    std::vector<uint8_t> cls(static_cast<size_t>(R * C), UNSET);
+    auto mark = [&](const int64_t* ij, int64_t n, uint8_t c, const char* name) -> bool {
+        if (n > 0 && !ij) { why = std::string(name) + " list is NULL"; return false; }
+        for (int64_t q = 0; q < n; ++q) {
+            const int64_t i = ij[2 * q], j = ij[2 * q + 1];
+            if (i < 0 || j < 0 || i >= R || j >= C) { why = std::string(name) + " node out of range"; return false; }
+            uint8_t& s = cls[static_cast<size_t>(i + R * j)];
+            if (s != UNSET) { why = std::string(name) + " node also listed as another node kind"; return false; }
+            s = c;
+        }
+        return true;
+    };
+    // provisional codes: 1 fluid, 2 wall/obstacle, 3 inlet, 4 outlet
+    if (!mark(d->fluid_ij, d->n_fluid, 1, "fluid") || !mark(d->wall_ij, d->n_wall, 2, "wall") ||
+        !mark(d->inlet_ij, d->n_inlet, 3, "inlet") || !mark(d->outlet_ij, d->n_outlet, 4, "outlet") ||
+        !mark(d->obstacle_ij, d->n_obstacle, 2, "obstacle"))
+        return LLB_E_GEOMETRY;
+    auto at = [&](int64_t i, int64_t j) -> uint8_t {
+        if (i < 0 || j < 0 || i >= R || j >= C) return UNSET;
+        return cls[static_cast<size_t>(i + R * j)];
+    };
+    auto active = [](uint8_t c) { return c == 1 || c == 3 || c == 4; };
+    // The reference streams fluid nodes without bounds checks; a fluid node on
+    // the lattice edge would write outside its tensors.
+    for (int64_t q = 0; q < d->n_fluid; ++q) {
+        const int64_t i = d->fluid_ij[2 * q], j = d->fluid_ij[2 * q + 1];
+        if (i == 0 || j == 0 || i == R - 1 || j == C - 1) {
+            why = "fluid node on the lattice edge (the reference streams it out of bounds)";
+            return LLB_E_GEOMETRY;
+        }
+    }
+    // obstacle direction bits must be the reference's rule (bit k iff x + c_k active)
+    if (d->obstacle_dirs) {
+        for (int64_t q = 0; q < d->n_obstacle; ++q) {
+            const int64_t i = d->obstacle_ij[2 * q], j = d->obstacle_ij[2 * q + 1];
+            uint16_t b = 0;
+            for (int k = 1; k < 9; ++k)
+                if (active(at(i + DI(k), j + DJ(k)))) b |= static_cast<uint16_t>(1u << k);
+            if (b != (d->obstacle_dirs[q] & 0x1feu)) {
+                why = "obstacle direction bits differ from the neighbour rule of identify_obstacle_propagation";
+                return LLB_E_UNSUPPORTED;
+            }
+        }
+    }
+    mask.assign(static_cast<size_t>(ld) * C, 0);
+    open_idx.assign(static_cast<size_t>(ld) * C, -1);
+    auto side_code = [](int32_t bt) { return (bt >= 1 && bt <= 4) ? bt : SIDE_NONE; };
+    for (int64_t j = 0; j < C; ++j) {
+        for (int64_t i = 0; i < R; ++i) {
+            const uint8_t c = at(i, j);
+            uint8_t m = CLS_DEAD;
+            if (c == 1) m = CLS_FLUID;
+            else if (c == 2) m = CLS_BB;
+            else if (c == 3 || c == 4) m = CLS_OPEN;
+            if (active(c)) {
+                bool plain = true;
+                for (int k = 1; k < 9; ++k)
+                    if (!active(at(i - DI(k), j - DJ(k)))) plain = false;
+                if (plain) m |= MASK_PLAIN;
+            }
+            mask[static_cast<size_t>(j * ld + i)] = m;
+        }
+    }
+    auto set_open = [&](const int64_t* ij, const int32_t* side, int64_t n, int bc, int base) {
+        for (int64_t q = 0; q < n; ++q) {
+            const int64_t i = ij[2 * q], j = ij[2 * q + 1];
+            const size_t x = static_cast<size_t>(j * ld + i);
+            const int s = side ? side_code(side[q]) : SIDE_NONE;
+            mask[x] = static_cast<uint8_t>((mask[x] & 7u) | (s << SIDE_SHIFT) | (bc << BC_SHIFT));
+            open_idx[x] = static_cast<int32_t>(base + q);
+        }
+    };
+    set_open(d->inlet_ij, d->inlet_side, d->n_inlet, d->inlet_bc, 0);
+    set_open(d->outlet_ij, d->outlet_side, d->n_outlet, d->outlet_bc, static_cast<int>(d->n_inlet));
+    return LLB_OK;
+}
+
+int ensure_partials(llb_handle h, int nblocks) {
+    if (h->partial_blocks >= nblocks) return LLB_OK;
+    if (h->d_partials) { cudaFree(h->d_partials); h->d_partials = nullptr; }
+    int rc = dev_alloc(h, &h->d_partials, sizeof(double2) * 3 * static_cast<size_t>(nblocks));
+    if (rc) return rc;
+    h->partial_blocks = nblocks;
+    return LLB_OK;
+}
+
+int launch_one(llb_handle h, bool macro) {
+    LaunchCtx x = make_ctx(h);
+    cudaError_t e = launch_step(h->storage, x, h->f[h->cur], h->f[h->cur ^ 1], false, macro);
+    if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
+    h->cur ^= 1;
+    ++h->step;
+    return LLB_OK;
+}
+
+int graph_for(llb_handle h, cudaGraphExec_t* out) {
+    if (h->graph[h->cur]) { *out = h->graph[h->cur]; return LLB_OK; }
+    const int cur0 = h->cur;
+    const int64_t step0 = h->step;
+    cudaGraph_t g = nullptr;
+    LLB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = LLB_OK;
+    for (int s = 0; s < GRAPH_STEPS && rc == LLB_OK; ++s) rc = launch_one(h, false);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->cur = cur0;
+    h->step = step0;
+    if (rc != LLB_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&h->graph[cur0], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    *out = h->graph[cur0];
+    return LLB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// dispatch to the storage-specific translation units
+// ---------------------------------------------------------------------------
+namespace llb {
+cudaError_t launch_step(int s, const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
+    return s == LLB_STORE_F64 ? launch_step_f64(x, fin, fout, init, macro) : launch_step_lowp(s, x, fin, fout, init, macro);
+}
+cudaError_t launch_finalize(int s, const LaunchCtx& x, const void* fin, double* out, long long t) {
+    return s == LLB_STORE_F64 ? launch_finalize_f64(x, fin, out, t) : launch_finalize_lowp(s, x, fin, out, t);
+}
+cudaError_t launch_export(int s, const LaunchCtx& x, const void* fin, double* out) {
+    return s == LLB_STORE_F64 ? launch_export_f64(x, fin, out) : launch_export_lowp(s, x, fin, out);
+}
+cudaError_t launch_mass_momentum(int s, const LaunchCtx& x, const void* fin, double2* p, int nb, double* out3) {
+    return s == LLB_STORE_F64 ? launch_mass_momentum_f64(x, fin, p, nb, out3) : launch_mass_momentum_lowp(s, x, fin, p, nb, out3);
+}
+cudaError_t launch_flow_forces(int s, const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
+                               long long n, double2* p, int nb, double* out2) {
+    return s == LLB_STORE_F64 ? launch_flow_forces_f64(x, fin, pts, dirs, n, p, nb, out2)
+                              : launch_flow_forces_lowp(s, x, fin, pts, dirs, n, p, nb, out2);
+}
+cudaError_t launch_gather_forces(int s, const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
+                                 long long n, double* out) {
+    return s == LLB_STORE_F64 ? launch_gather_forces_f64(x, fin, pts, dirs, n, out)
+                              : launch_gather_forces_lowp(s, x, fin, pts, dirs, n, out);
+}
+}  // namespace llb
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int llb_abi_version(void) { return LLB_ABI_VERSION; }
+
+const char* llb_last_error(llb_handle h) { return h ? h->err.c_str() : g_last_error.c_str(); }
+
+int llb_create(const llb_desc* d, llb_handle* out) {
+    if (!d || !out) return fail(nullptr, LLB_E_INVALID, "null descriptor or output");
+    *out = nullptr;
+    if (d->rows < 3 || d->cols < 3 || d->rows > (1 << 30) || d->cols > (1 << 30) || d->rows * d->cols > (1LL << 36))
+        return fail(nullptr, LLB_E_INVALID, "lattice dimensions out of range");
+    if (d->n_fluid < 0 || d->n_wall < 0 || d->n_inlet < 0 || d->n_outlet < 0 || d->n_obstacle < 0)
+        return fail(nullptr, LLB_E_INVALID, "negative node count");
+    if (d->collision != LLB_BGK && d->collision != LLB_TRT) return fail(nullptr, LLB_E_INVALID, "bad collision");
+    if (d->storage < LLB_STORE_F64 || d->storage > LLB_STORE_F16S) return fail(nullptr, LLB_E_INVALID, "bad storage");
+    if (d->pattern != LLB_PATTERN_AB && d->pattern != LLB_PATTERN_AA) return fail(nullptr, LLB_E_INVALID, "bad pattern");
+    if (d->pattern == LLB_PATTERN_AA) return fail(nullptr, LLB_E_UNSUPPORTED, "A-A pattern not available in this build");
+    for (int bc : {d->inlet_bc, d->outlet_bc})
+        if (bc < LLB_BC_ZH_VELOCITY || bc > LLB_BC_ZH_PRESSURE) return fail(nullptr, LLB_E_INVALID, "bad boundary policy");
+    if (d->collision == LLB_BGK && !(d->tau > 0.0)) return fail(nullptr, LLB_E_INVALID, "tau must be > 0");
+    if (d->collision == LLB_TRT && !(d->tau_even > 0.0 && d->tau_odd > 0.0))
+        return fail(nullptr, LLB_E_INVALID, "tau_even and tau_odd must be > 0");
+    const int64_t n_open = d->n_inlet + d->n_outlet;
+    if (n_open > (1LL << 30)) return fail(nullptr, LLB_E_INVALID, "too many open nodes");
+    const int cap = d->open_table_rows <= 0 ? 1 : d->open_table_rows;
+
+    llb_handle h = new (std::nothrow) llb_lattice();
+    if (!h) return fail(nullptr, LLB_E_NOMEM, "host allocation failed");
+    h->device = d->device;
+    h->storage = d->storage;
+    h->pattern = d->pattern;
+    h->R = d->rows;
+    h->C = d->cols;
+    h->elem = d->storage == LLB_STORE_F64 ? 8 : (d->storage == LLB_STORE_F32S ? 4 : 2);
+    const int align = static_cast<int>(256 / h->elem);  // every column starts 256-byte aligned
+    h->ld = static_cast<int>((d->rows + align - 1) / align * align);
+    h->plane = static_cast<long long>(h->ld) * d->cols;
+    h->n_open = static_cast<int>(n_open);
+    h->cap = cap;
+    if (d->collision == LLB_BGK) {
+        h->coll.model = 0;
+        h->coll.t = 1.0 / d->tau;  // BGKCollision.hpp:142-143
+        h->coll.omt = 1.0 - h->coll.t;
+    } else {
+        h->coll.model = 1;
+        h->coll.ie = 1.0 / d->tau_even;  // TRTCollision.hpp:155-188
+        h->coll.he = 0.5 * (1.0 / d->tau_even);
+        h->coll.ho = 0.5 * (1.0 / d->tau_odd);
+    }
+
+    std::vector<uint8_t> mask;
+    std::vector<int32_t> open_idx;
+    std::string why;
+    int rc = build_mask(d, h->ld, mask, open_idx, why);
+    if (rc != LLB_OK) { delete h; return fail(nullptr, rc, why); }
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete h; return fail(nullptr, LLB_E_NODEVICE, "no CUDA device"); }
+    if (d->device < 0 || d->device >= ndev) { delete h; return fail(nullptr, LLB_E_NODEVICE, "device ordinal out of range"); }
+
+    auto bail = [&](int code) { std::string m = h->err; release(h); return fail(nullptr, code, m); };
+    if ((rc = select_device(h))) return bail(rc);
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaStreamCreate"));
+    const size_t pop_bytes = static_cast<size_t>(h->plane) * 9 * h->elem;
+    const size_t N = static_cast<size_t>(h->R * h->C);
+    if ((rc = dev_alloc(h, &h->f[0], pop_bytes)) || (rc = dev_alloc(h, &h->f[1], pop_bytes)) ||
+        (rc = dev_alloc(h, &h->d_mask, mask.size())) ||
+        (rc = dev_alloc(h, &h->d_open_idx, open_idx.size() * sizeof(int32_t))) ||
+        (rc = dev_alloc(h, &h->d_open, sizeof(double2) * static_cast<size_t>(std::max<int64_t>(n_open, 1)) * cap)) ||
+        (rc = dev_alloc(h, &h->d_rho, sizeof(double) * N)) || (rc = dev_alloc(h, &h->d_u, sizeof(double) * 2 * N)) ||
+        (rc = dev_alloc(h, &h->d_step, sizeof(long long))) || (rc = dev_alloc(h, &h->d_done, sizeof(unsigned))) ||
+        (rc = dev_alloc(h, &h->d_flags, sizeof(unsigned))) || (rc = dev_alloc(h, &h->d_red, sizeof(double) * 4)))
+        return bail(rc);
+    e = cudaMemcpyAsync(h->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->d_open_idx, open_idx.data(), open_idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(h->d_open, 0, sizeof(double2) * static_cast<size_t>(std::max<int64_t>(n_open, 1)) * cap, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->f[0], 0, pop_bytes, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->f[1], 0, pop_bytes, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_done, 0, sizeof(unsigned), h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return bail(cuda_fail(h, e, "lattice upload"));
+    *out = h;
+    return LLB_OK;
+}
+
+int llb_destroy(llb_handle h) {
+    if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
+    release(h);
+    return LLB_OK;
+}
+
+int llb_set_open_values(llb_handle h, int64_t t_first, int32_t count, const double* values) {
+    if (!h || t_first < 0 || count < 0) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (h->n_open == 0 || count == 0) return LLB_OK;
+    if (!values) return fail(h, LLB_E_INVALID, "null values");
+    if (count > h->cap) return fail(h, LLB_E_INVALID, "more rows than the open-value ring holds");
+    int rc = select_device(h);
+    if (rc) return rc;
+    const size_t row = sizeof(double2) * static_cast<size_t>(h->n_open);
+    int32_t r = 0;
+    while (r < count) {
+        const int64_t slot = (t_first + r) % h->cap;
+        const int32_t run = static_cast<int32_t>(std::min<int64_t>(count - r, h->cap - slot));
+        LLB_CUDA(h, cudaMemcpyAsync(reinterpret_cast<char*>(h->d_open) + slot * row,
+                                    reinterpret_cast<const char*>(values) + static_cast<size_t>(r) * row, row * run,
+                                    cudaMemcpyHostToDevice, h->stream));
+        r += run;
+    }
+    return LLB_OK;
+}
+
+int llb_init(llb_handle h, uint32_t flags) {
+    if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
+    int rc = select_device(h);
+    if (rc) return rc;
+    LLB_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
+    LLB_CUDA(h, cudaMemsetAsync(h->d_done, 0, sizeof(unsigned), h->stream));
+    h->cur = 0;
+    LaunchCtx x = make_ctx(h);
+    const bool macro = (flags & LLB_STEP_MACRO) != 0;
+    cudaError_t e = launch_step(h->storage, x, nullptr, h->f[0], true, macro);
+    if (e != cudaSuccess) return cuda_fail(h, e, "init kernel launch");
+    h->step = 1;
+    h->initialized = true;
+    h->macro_valid = macro;
+    return LLB_OK;
+}
+
+int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
+    if (!h || nsteps < 0) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "llb_step before llb_init");
+    if (nsteps == 0) return LLB_OK;
+    int rc = select_device(h);
+    if (rc) return rc;
+    const bool macro = (flags & LLB_STEP_MACRO) != 0;
+    int32_t plain = macro ? nsteps - 1 : nsteps;
+    if (plain >= GRAPH_STEPS) {
+        cudaGraphExec_t g = nullptr;
+        if ((rc = graph_for(h, &g))) return rc;
+        while (plain >= GRAPH_STEPS) {
+            LLB_CUDA(h, cudaGraphLaunch(g, h->stream));
+            h->step += GRAPH_STEPS;
+            plain -= GRAPH_STEPS;
+        }
+    }
+    for (int32_t s = 0; s < plain; ++s)
+        if ((rc = launch_one(h, false))) return rc;
+    if (macro) {
+        if ((rc = launch_one(h, true))) return rc;
+        h->macro_valid = true;
+    }
+    return LLB_OK;
+}
+
+int llb_get_step(llb_handle h, int64_t* step) {
+    if (!h || !step) return fail(h, LLB_E_INVALID, "bad arguments");
+    *step = h->step;
+    return LLB_OK;
+}
+
+int llb_get_macro(llb_handle h, double* rho, double* u) {
+    if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
+    if (!h->macro_valid) return fail(h, LLB_E_STATE, "no step has written rho/u yet");
+    int rc = select_device(h);
+    if (rc) return rc;
+    const size_t N = static_cast<size_t>(h->R * h->C);
+    if (rho) LLB_CUDA(h, cudaMemcpyAsync(rho, h->d_rho, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
+    if (u) LLB_CUDA(h, cudaMemcpyAsync(u, h->d_u, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+static int dense_out(llb_handle h, double* host, bool finalize) {
+    if (!h || !host) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
+    int rc = select_device(h);
+    if (rc) return rc;
+    const size_t bytes = sizeof(double) * 9 * static_cast<size_t>(h->R * h->C);
+    if (!h->d_dense && (rc = dev_alloc(h, &h->d_dense, bytes))) return rc;
+    LaunchCtx x = make_ctx(h);
+    cudaError_t e = finalize ? launch_finalize(h->storage, x, h->f[h->cur], h->d_dense, h->step)
+                             : launch_export(h->storage, x, h->f[h->cur], h->d_dense);
+    if (e != cudaSuccess) return cuda_fail(h, e, "export kernel launch");
+    LLB_CUDA(h, cudaMemcpyAsync(host, h->d_dense, bytes, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_get_populations(llb_handle h, double* populations) { return dense_out(h, populations, true); }
+int llb_get_post_collision(llb_handle h, double* populations) { return dense_out(h, populations, false); }
+
+int llb_set_force_points(llb_handle h, const int64_t* ij, const uint16_t* dirs, int64_t n) {
+    if (!h || n < 0 || (n > 0 && (!ij || !dirs))) return fail(h, LLB_E_INVALID, "bad arguments");
+    for (int64_t q = 0; q < n; ++q)
+        if (ij[2 * q] < 0 || ij[2 * q + 1] < 0 || ij[2 * q] >= h->R || ij[2 * q + 1] >= h->C)
+            return fail(h, LLB_E_INVALID, "force point out of range");
+    int rc = select_device(h);
+    if (rc) return rc;
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (void* p : {static_cast<void*>(h->d_fpts), static_cast<void*>(h->d_fdirs), static_cast<void*>(h->d_gather)})
+        if (p) cudaFree(p);
+    h->d_fpts = nullptr;
+    h->d_fdirs = nullptr;
+    h->d_gather = nullptr;
+    h->n_fpts = n;
+    if (n == 0) return LLB_OK;
+    if ((rc = dev_alloc(h, &h->d_fpts, sizeof(int64_t) * 2 * n)) || (rc = dev_alloc(h, &h->d_fdirs, sizeof(uint16_t) * n)) ||
+        (rc = dev_alloc(h, &h->d_gather, sizeof(double) * 8 * n)))
+        return rc;
+    LLB_CUDA(h, cudaMemcpyAsync(h->d_fpts, ij, sizeof(int64_t) * 2 * n, cudaMemcpyHostToDevice, h->stream));
+    LLB_CUDA(h, cudaMemcpyAsync(h->d_fdirs, dirs, sizeof(uint16_t) * n, cudaMemcpyHostToDevice, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_flow_forces(llb_handle h, double lift_drag[2]) {
+    if (!h || !lift_drag) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
+    int rc = select_device(h);
+    if (rc) return rc;
+    const int nb = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(148 * 4, (h->n_fpts + 255) / 256)));
+    if ((rc = ensure_partials(h, nb))) return rc;
+    LaunchCtx x = make_ctx(h);
+    cudaError_t e = launch_flow_forces(h->storage, x, h->f[h->cur], h->d_fpts, h->d_fdirs, h->n_fpts, h->d_partials, nb, h->d_red);
+    if (e != cudaSuccess) return cuda_fail(h, e, "force kernel launch");
+    LLB_CUDA(h, cudaMemcpyAsync(lift_drag, h->d_red, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_gather_force_inputs(llb_handle h, double* values) {
+    if (!h || (h->n_fpts > 0 && !values)) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
+    if (h->n_fpts == 0) return LLB_OK;
+    int rc = select_device(h);
+    if (rc) return rc;
+    LaunchCtx x = make_ctx(h);
+    cudaError_t e = launch_gather_forces(h->storage, x, h->f[h->cur], h->d_fpts, h->d_fdirs, h->n_fpts, h->d_gather);
+    if (e != cudaSuccess) return cuda_fail(h, e, "gather kernel launch");
+    LLB_CUDA(h, cudaMemcpyAsync(values, h->d_gather, sizeof(double) * 8 * h->n_fpts, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_mass_momentum(llb_handle h, double out[3]) {
+    if (!h || !out) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
+    int rc = select_device(h);
+    if (rc) return rc;
+    const int64_t N = h->R * h->C;
+    const int nb = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(148 * 8, (N + 255) / 256)));
+    if ((rc = ensure_partials(h, nb))) return rc;
+    LaunchCtx x = make_ctx(h);
+    cudaError_t e = launch_mass_momentum(h->storage, x, h->f[h->cur], h->d_partials, nb, h->d_red);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reduction kernel launch");
+    LLB_CUDA(h, cudaMemcpyAsync(out, h->d_red, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_synchronize(llb_handle h) {
+    if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
+    int rc = select_device(h);
+    if (rc) return rc;
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_check_numerics(llb_handle h) {
+    if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
+    int rc = select_device(h);
+    if (rc) return rc;
+    unsigned flags = 0;
+    LLB_CUDA(h, cudaMemcpyAsync(&flags, h->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (flags & 1u) return fail(h, LLB_E_NUMERIC, "non-finite density detected");
+    return LLB_OK;
+}
+
+int llb_event_record(llb_handle h, int32_t slot) {
+    if (!h || slot < 0 || slot >= 8) return fail(h, LLB_E_INVALID, "bad arguments");
+    int rc = select_device(h);
+    if (rc) return rc;
+    if (!h->ev[slot]) LLB_CUDA(h, cudaEventCreate(&h->ev[slot]));
+    LLB_CUDA(h, cudaEventRecord(h->ev[slot], h->stream));
+    return LLB_OK;
+}
+
+int llb_event_elapsed_ms(llb_handle h, int32_t a, int32_t b, float* ms) {
+    if (!h || !ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !h->ev[a] || !h->ev[b])
+        return fail(h, LLB_E_INVALID, "bad arguments");
+    int rc = select_device(h);
+    if (rc) return rc;
+    LLB_CUDA(h, cudaEventSynchronize(h->ev[b]));
+    LLB_CUDA(h, cudaEventElapsedTime(ms, h->ev[a], h->ev[b]));
+    return LLB_OK;
+}
+
+int llb_device_bytes(llb_handle h, int64_t* bytes) {
+    if (!h || !bytes) return fail(h, LLB_E_INVALID, "bad arguments");
+    *bytes = h->bytes;
+    return LLB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,27 @@
+// FP64 kernels.  This translation unit is compiled with --fmad=false so that no
+// multiply and add are fused: the arithmetic then rounds exactly like the
+// reference's default x86-64 build, and results match it bit for bit.
+#include "llb_kernel_inst.cuh"
+
+namespace llb {
+
+cudaError_t launch_step_f64(const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
+    return do_step<ModelF64>(x, fin, fout, init, macro);
+}
+cudaError_t launch_finalize_f64(const LaunchCtx& x, const void* fin, double* out, long long t) {
+    return do_finalize<ModelF64>(x, fin, out, t);
+}
+cudaError_t launch_export_f64(const LaunchCtx& x, const void* fin, double* out) { return do_export<ModelF64>(x, fin, out); }
+cudaError_t launch_mass_momentum_f64(const LaunchCtx& x, const void* fin, double2* p, int nb, double* out3) {
+    return do_mass<ModelF64>(x, fin, p, nb, out3);
+}
+cudaError_t launch_flow_forces_f64(const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
+                                   long long n, double2* p, int nb, double* out2) {
+    return do_forces<ModelF64>(x, fin, pts, dirs, n, p, nb, out2);
+}
+cudaError_t launch_gather_forces_f64(const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
+                                     long long n, double* out) {
+    return do_gather<ModelF64>(x, fin, pts, dirs, n, out);
+}
+
+}  // namespace llb

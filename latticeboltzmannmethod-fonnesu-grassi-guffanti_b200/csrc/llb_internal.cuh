@@ -1,0 +1,100 @@
+// Internal definitions shared by the engine's translation units.
+//
+// Data layout in HBM (one lattice):
+//   populations : 9 planes, plane k at base + k*plane, node (i, j) at j*ld + i
+//                 (column-major like the reference's Eigen tensors, row index
+//                 fastest; ld = rows rounded up so every column starts on a
+//                 256-byte boundary).  Two such buffers (AB) or one (AA).
+//   mask        : one byte per node, same (j*ld + i) indexing.
+//   open_idx    : int32 per node, index of an inlet/outlet node in the open
+//                 value table (read only for open nodes).
+//   open_vals   : ring of [cap][n_open] double2 per-step boundary values.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+
+namespace llb {
+
+// ---- node mask byte ----------------------------------------------------------
+// bits 0-1  class: DEAD (never updated; as a streaming source its slot keeps the
+//           initial value), FLUID, BB (wall or wet obstacle: as a source it
+//           bounces the population back), OPEN (inlet or outlet)
+// bit  2    PLAIN: all 8 streaming sources are FLUID or OPEN (no per-direction
+//           source inspection needed)
+// bits 3-5  side of an OPEN node: 0 none/corner, 1 top, 2 right, 3 bottom, 4 left
+//           (the reference's btypes TOP_WALL..LEFT_WALL)
+// bits 6-7  closure of an OPEN node: 0 Zou-He velocity, 1 none, 2 Zou-He pressure
+constexpr uint8_t CLS_DEAD = 0, CLS_FLUID = 1, CLS_BB = 2, CLS_OPEN = 3;
+constexpr uint8_t MASK_PLAIN = 4;
+constexpr int SIDE_SHIFT = 3, BC_SHIFT = 6;
+constexpr int SIDE_NONE = 0, SIDE_TOP = 1, SIDE_RIGHT = 2, SIDE_BOTTOM = 3, SIDE_LEFT = 4;
+constexpr int BC_ZH_VEL = 0, BC_OPEN = 1, BC_ZH_PRES = 2;
+
+__host__ __device__ constexpr uint8_t mask_class(uint8_t m) { return m & 3u; }
+__host__ __device__ constexpr int mask_side(uint8_t m) { return (m >> SIDE_SHIFT) & 7; }
+__host__ __device__ constexpr int mask_bc(uint8_t m) { return (m >> BC_SHIFT) & 3; }
+__host__ __device__ constexpr bool class_active(uint8_t c) { return c == CLS_FLUID || c == CLS_OPEN; }
+
+// D2Q9 directions as (di, dj) of the reference's push (BGKCollision.hpp:179-187):
+// 1 (0,+1) 2 (-1,0) 3 (0,-1) 4 (+1,0) 5 (-1,+1) 6 (-1,-1) 7 (+1,-1) 8 (+1,+1).
+// A pull reads direction k from the node at (i - di, j - dj).
+__host__ __device__ constexpr int DI(int k) {
+    return k == 2 || k == 5 || k == 6 ? -1 : (k == 4 || k == 7 || k == 8 ? 1 : 0);
+}
+__host__ __device__ constexpr int DJ(int k) {
+    return k == 1 || k == 5 || k == 8 ? 1 : (k == 3 || k == 6 || k == 7 ? -1 : 0);
+}
+// opposite directions 1<->3, 2<->4, 5<->7, 6<->8
+__host__ __device__ constexpr int opp(int k) {
+    return k == 1 ? 3 : k == 2 ? 4 : k == 3 ? 1 : k == 4 ? 2 : k == 5 ? 7 : k == 6 ? 8 : k == 7 ? 5 : k == 8 ? 6 : 0;
+}
+
+// Initial populations of every active node: the reference's equilibrium at
+// rho = 1, u = 0 (Lattice.hpp:326-328 with DefaultEquilibrium.hpp:64-76),
+// evaluated with the same expressions.  A population slot nobody streams into
+// keeps this value for the whole run.
+__host__ __device__ constexpr double w_init(int k) {
+    return k == 0 ? (2.0 / 9.0) * 1.0 * (2 - 3 * 0.0)
+         : k <= 4 ? (1.0 / 18.0) * 1.0 * (2 + 6 * 0.0 + 9 * 0.0 * 0.0 - 3 * 0.0)
+                  : (1.0 / 36.0) * 1.0 * (1 + 3 * (0.0 + 0.0) + 9 * 0.0 * 0.0 + 3 * 0.0);
+}
+// Lattice weights used by the shifted (f - w) storage forms.
+__host__ __device__ constexpr float w_f32(int k) { return k == 0 ? 4.0f / 9.0f : (k <= 4 ? 1.0f / 9.0f : 1.0f / 36.0f); }
+
+// ---- kernel parameters ------------------------------------------------------
+struct Geometry {
+    int rows, cols;     // R, C
+    int ld;             // column stride (elements) of populations / mask / open_idx
+    long long plane;    // ld * cols
+    const uint8_t* __restrict__ mask;
+    const int32_t* __restrict__ open_idx;
+};
+
+struct OpenTable {
+    const double2* __restrict__ vals;  // [cap][n_open]
+    int n_open;
+    int cap;
+};
+
+struct Collision {
+    int model;          // 0 BGK, 1 TRT
+    // BGK: t = 1/tau, omt = 1 - t   (BGKCollision.hpp:142-143)
+    double t, omt;
+    // TRT: ie = 1/tau_even, he = 0.5*(1/tau_even), ho = 0.5*(1/tau_odd)   (TRTCollision.hpp:155-188)
+    double ie, he, ho;
+};
+
+struct MacroOut {
+    double* rho;        // (R, C) dense, column-major
+    double* u;          // (R, C, 2) dense
+};
+
+struct StepSync {
+    long long* step;    // device step counter (index of the step being computed)
+    unsigned* done;     // blocks finished in the current launch
+    unsigned* flags;    // bit 0: non-finite density seen
+};
+
+}  // namespace llb

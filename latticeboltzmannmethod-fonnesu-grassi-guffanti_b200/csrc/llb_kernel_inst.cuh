@@ -1,0 +1,64 @@
+// Launch wrappers for one storage model M (included by llb_f64.cu and llb_lowp.cu).
+#pragma once
+
+#include "llb_kernels.cuh"
+#include "llb_launch.h"
+
+namespace llb {
+
+template <class M>
+cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
+    using T = typename M::T;
+    const dim3 block(BX, BY), grid = node_grid(x.g, BX, BY);
+    const T* in = static_cast<const T*>(fin);
+    T* out = static_cast<T*>(fout);
+#define LLB_STEP(COLL, MAC, INI) k_step<M, COLL, MAC, INI><<<grid, block, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss)
+    if (x.c.model == 0) {
+        if (init) { if (macro) LLB_STEP(0, true, true); else LLB_STEP(0, false, true); }
+        else { if (macro) LLB_STEP(0, true, false); else LLB_STEP(0, false, false); }
+    } else {
+        if (init) { if (macro) LLB_STEP(1, true, true); else LLB_STEP(1, false, true); }
+        else { if (macro) LLB_STEP(1, true, false); else LLB_STEP(1, false, false); }
+    }
+#undef LLB_STEP
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_finalize(const LaunchCtx& x, const void* fin, double* out, long long t) {
+    k_finalize<M><<<node_grid(x.g, BX, BY), dim3(BX, BY), 0, x.stream>>>(
+        x.g, x.ot, static_cast<const typename M::T*>(fin), out, t);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_export(const LaunchCtx& x, const void* fin, double* out) {
+    k_export<M><<<node_grid(x.g, BX, BY), dim3(BX, BY), 0, x.stream>>>(x.g, static_cast<const typename M::T*>(fin), out);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_mass(const LaunchCtx& x, const void* fin, double2* partials, int nblocks, double* out3) {
+    k_mass_momentum<M><<<nblocks, 256, 0, x.stream>>>(x.g, static_cast<const typename M::T*>(fin), partials);
+    k_reduce_partials<3><<<1, 32, 0, x.stream>>>(partials, nblocks, out3);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_forces(const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs, long long n,
+                      double2* partials, int nblocks, double* out2) {
+    k_flow_forces<M><<<nblocks, 256, 0, x.stream>>>(x.g, static_cast<const typename M::T*>(fin), pts, dirs, n, partials);
+    k_reduce_partials<2><<<1, 32, 0, x.stream>>>(partials, nblocks, out2);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_gather(const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs, long long n,
+                      double* out) {
+    if (n <= 0) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+    k_gather_forces<M><<<blocks, 256, 0, x.stream>>>(x.g, static_cast<const typename M::T*>(fin), pts, dirs, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace llb

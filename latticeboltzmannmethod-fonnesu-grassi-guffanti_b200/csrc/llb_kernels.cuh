@@ -1,0 +1,346 @@
+// Kernel skeletons shared by every storage form (instantiated in llb_f64.cu and
+// llb_lowp.cu).  One thread owns one node; a block is 32 consecutive rows of 8
+// consecutive columns, so a warp reads and writes 32 contiguous entries of each
+// population plane.
+//
+// The resident state is the post-collision populations f*.  One step t computes,
+// for every fluid, inlet and outlet node x:
+//   1. pull  S_t(x,k):  f*_{t-1}(x - c_k, k)   if the source node is fluid or open
+//                       f*_{t-1}(x, opp(k))    if it is a wall or wet obstacle
+//                                              (half-way bounce-back)
+//                       initial value w_k      if outside the lattice or dead
+//      -- the reference's push stream + bounce-back (Lattice.hpp:393-403) seen
+//         from the receiving node: every population slot has exactly one writer;
+//   2. the inlet/outlet closure with the boundary values of step t-1
+//      (Lattice.hpp:409-410, run at the end of the reference's iteration t-1);
+//   3. moments of fluid nodes, boundary values of step t for open nodes
+//      (update_nodes + update_macro, Lattice.hpp:351-357);
+//   4. equilibrium and collision (Lattice.hpp:363-382), store f*_t.
+#pragma once
+
+#include "llb_model.cuh"
+
+namespace llb {
+
+constexpr int BX = 32, BY = 8;
+
+template <class M>
+__device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __restrict__ fin, int i, int j,
+                                     long long node, uint8_t m, typename M::R* f) {
+    f[0] = M::load(fin + node);
+    if (m & MASK_PLAIN) {
+#pragma unroll
+        for (int k = 1; k < 9; ++k)
+            f[k] = M::load(fin + k * g.plane + node - (DJ(k) * g.ld + DI(k)));
+    } else {
+#pragma unroll
+        for (int k = 1; k < 9; ++k) {
+            const int si = i - DI(k), sj = j - DJ(k);
+            typename M::R v = M::keep(k);
+            if (si >= 0 && sj >= 0 && si < g.rows && sj < g.cols) {
+                const long long src = static_cast<long long>(sj) * g.ld + si;
+                const uint8_t sc = mask_class(g.mask[src]);
+                if (class_active(sc)) v = M::load(fin + k * g.plane + src);
+                else if (sc == CLS_BB) v = M::load(fin + opp(k) * g.plane + node);
+            }
+            f[k] = v;
+        }
+    }
+}
+
+// Closure + choice of (rho, u) for an open node at step t (t >= 1), or for the
+// initial step (t == 0: no closure, pressure nodes start at rest).
+template <class M>
+__device__ __forceinline__ void open_node(const OpenTable& ot, int q, uint8_t m, long long t, typename M::R* f,
+                                          double& rho, double& ux, double& uy) {
+    const int side = mask_side(m), bc = mask_bc(m);
+    const double2 cur = ot.vals[static_cast<long long>(t % ot.cap) * ot.n_open + q];
+    if (bc == BC_ZH_PRES) {
+        rho = cur.x;
+        if (t == 0) {
+            ux = 0.0;
+            uy = 0.0;
+        } else {
+            const double2 prev = ot.vals[static_cast<long long>((t - 1) % ot.cap) * ot.n_open + q];
+            M::closure_pressure(f, side, prev.x, prev.y, ux, uy);
+        }
+    } else {
+        if (bc == BC_ZH_VEL && t > 0) {
+            const double2 prev = ot.vals[static_cast<long long>((t - 1) % ot.cap) * ot.n_open + q];
+            M::closure_velocity(f, side, prev.x, prev.y);
+        }
+        rho = 1.0;  // open nodes collide with global_rho == 1 (never written for them)
+        ux = cur.x;
+        uy = cur.y;
+    }
+}
+
+__device__ __forceinline__ void finish_block(const StepSync& ss, long long t, bool bad) {
+    const unsigned full = 0xffffffffu;
+    if (__any_sync(full, bad) && (threadIdx.x & 31) == 0) atomicOr(ss.flags, 1u);
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        const unsigned total = gridDim.x * gridDim.y;
+        const unsigned prev = atomicAdd(ss.done, 1u);
+        if (prev == total - 1) {
+            *ss.done = 0u;
+            *ss.step = t + 1;
+            __threadfence();
+        }
+    }
+}
+
+// INIT == true: step 0 from the initial equilibrium (Lattice.hpp:326-328).
+template <class M, int COLL, bool MACRO, bool INIT>
+__global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Collision c,
+                                                 const typename M::T* __restrict__ fin,
+                                                 typename M::T* __restrict__ fout, MacroOut mo, StepSync ss) {
+    const long long t = INIT ? 0 : *reinterpret_cast<volatile long long*>(ss.step);
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    bool bad = false;
+    if (i < g.rows && j < g.cols) {
+        const long long node = static_cast<long long>(j) * g.ld + i;
+        const uint8_t m = g.mask[node];
+        const uint8_t cls = mask_class(m);
+        if (class_active(cls)) {
+            typename M::R f[9];
+            if (INIT) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) f[k] = M::keep(k);
+            } else {
+                pull<M>(g, fin, i, j, node, m, f);
+            }
+            double rho, ux, uy;
+            typename M::R rr;
+            if (cls == CLS_OPEN) {
+                open_node<M>(ot, g.open_idx[node], m, t, f, rho, ux, uy);
+                rr = M::from_f64(rho);
+            } else {
+                typename M::R r, x, y;
+                M::moments(f, r, x, y);
+                rr = r;
+                ux = x;
+                uy = y;
+                rho = M::rho_f64(r);
+                bad = !isfinite(rho);
+            }
+            if (MACRO) {
+                const long long d = static_cast<long long>(j) * g.rows + i;
+                const long long N = static_cast<long long>(g.rows) * g.cols;
+                mo.rho[d] = rho;
+                mo.u[d] = ux;
+                mo.u[d + N] = uy;
+            }
+            M::template collide<COLL>(f, rr, ux, uy, c);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
+        } else if (MACRO) {
+            const long long d = static_cast<long long>(j) * g.rows + i;
+            const long long N = static_cast<long long>(g.rows) * g.cols;
+            mo.rho[d] = 1.0;  // global_rho / global_u keep their initial values off active nodes
+            mo.u[d] = 0.0;
+            mo.u[d + N] = 0.0;
+        }
+    }
+    finish_block(ss, t, bad);
+}
+
+// populations S_t = stream + bounce-back + closures of the resident state,
+// written as a dense (R, C, 9) FP64 tensor (0 off active nodes).
+template <class M>
+__global__ void __launch_bounds__(BX* BY) k_finalize(Geometry g, OpenTable ot, const typename M::T* __restrict__ fin,
+                                                     double* __restrict__ out, long long t) {
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= g.rows || j >= g.cols) return;
+    const long long node = static_cast<long long>(j) * g.ld + i;
+    const long long d = static_cast<long long>(j) * g.rows + i;
+    const long long N = static_cast<long long>(g.rows) * g.cols;
+    const uint8_t m = g.mask[node];
+    const uint8_t cls = mask_class(m);
+    if (!class_active(cls)) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) out[d + k * N] = 0.0;
+        return;
+    }
+    typename M::R f[9];
+    pull<M>(g, fin, i, j, node, m, f);
+    if (cls == CLS_OPEN && t > 0) {
+        const int q = g.open_idx[node];
+        const double2 prev = ot.vals[static_cast<long long>((t - 1) % ot.cap) * ot.n_open + q];
+        if (mask_bc(m) == BC_ZH_VEL) M::closure_velocity(f, mask_side(m), prev.x, prev.y);
+        else if (mask_bc(m) == BC_ZH_PRES) {
+            double ux, uy;
+            M::closure_pressure(f, mask_side(m), prev.x, prev.y, ux, uy);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[d + k * N] = M::to_f64(f[k], k);
+}
+
+// after_collision_populations as a dense (R, C, 9) FP64 tensor.
+template <class M>
+__global__ void __launch_bounds__(BX* BY) k_export(Geometry g, const typename M::T* __restrict__ fin,
+                                                   double* __restrict__ out) {
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= g.rows || j >= g.cols) return;
+    const long long node = static_cast<long long>(j) * g.ld + i;
+    const long long d = static_cast<long long>(j) * g.rows + i;
+    const long long N = static_cast<long long>(g.rows) * g.cols;
+    const bool act = class_active(mask_class(g.mask[node]));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[d + k * N] = act ? M::to_f64(M::load(fin + k * g.plane + node), k) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// compensated FP64 reductions (Neumaier), deterministic order
+// ---------------------------------------------------------------------------
+struct Neu {
+    double s, c;
+};
+__device__ __forceinline__ Neu neu_add(Neu a, double x) {
+    const double t = a.s + x;
+    if (fabs(a.s) >= fabs(x)) a.c += (a.s - t) + x;
+    else a.c += (x - t) + a.s;
+    a.s = t;
+    return a;
+}
+__device__ __forceinline__ Neu neu_merge(Neu a, Neu b) {
+    Neu r = neu_add(a, b.s);
+    r.c += b.c;
+    return r;
+}
+
+// Block-wide reduction of NV compensated sums; thread 0 of the block writes
+// partials[blockIdx][v] = (s, c).  Fixed shuffle and warp order.
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(Neu (&acc)[NV], double2* partials) {
+    __shared__ Neu sh[32][NV];
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        for (int off = 16; off > 0; off >>= 1) {
+            Neu o;
+            o.s = __shfl_down_sync(0xffffffffu, acc[v].s, off);
+            o.c = __shfl_down_sync(0xffffffffu, acc[v].c, off);
+            if (lane + off < 32) acc[v] = neu_merge(acc[v], o);
+        }
+        if (lane == 0) sh[warp][v] = acc[v];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int v = 0; v < NV; ++v) {
+            Neu r = sh[0][v];
+            for (int w = 1; w < nwarps; ++w) r = neu_merge(r, sh[w][v]);
+            partials[static_cast<long long>(blockIdx.x) * NV + v] = make_double2(r.s, r.c);
+        }
+    }
+}
+
+// final pass: one block folds the per-block partials in index order
+template <int NV>
+__global__ void k_reduce_partials(const double2* __restrict__ partials, int nblocks, double* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    for (int v = 0; v < NV; ++v) {
+        Neu r{0.0, 0.0};
+        for (int b = 0; b < nblocks; ++b) {
+            const double2 p = partials[static_cast<long long>(b) * NV + v];
+            r = neu_merge(r, Neu{p.x, p.y});
+        }
+        out[v] = r.s + r.c;
+    }
+}
+
+// mass and momentum of the resident post-collision state over active nodes
+template <class M>
+__global__ void __launch_bounds__(256) k_mass_momentum(Geometry g, const typename M::T* __restrict__ fin,
+                                                       double2* partials) {
+    Neu acc[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    const long long N = static_cast<long long>(g.rows) * g.cols;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; x < N; x += stride) {
+        const int j = static_cast<int>(x / g.rows), i = static_cast<int>(x - static_cast<long long>(j) * g.rows);
+        const long long node = static_cast<long long>(j) * g.ld + i;
+        if (!class_active(mask_class(g.mask[node]))) continue;
+        double f[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) f[k] = M::to_f64(M::load(fin + k * g.plane + node), k);
+        const double m = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+        const double mx = (f[1] + f[5] + f[8]) - (f[3] + f[6] + f[7]);
+        const double my = (f[2] + f[5] + f[6]) - (f[4] + f[7] + f[8]);
+        acc[0] = neu_add(acc[0], m);
+        acc[1] = neu_add(acc[1], mx);
+        acc[2] = neu_add(acc[2], my);
+    }
+    block_reduce_store<3>(acc, partials);
+}
+
+// FlowAnalyzer<2>::compute_flow_properties (FlowAnalyzer.hpp:394-427): the value
+// of bit k is the neighbour x + c_k's population in direction opp(k).
+template <class M>
+__device__ __forceinline__ double force_input(const Geometry& g, const typename M::T* __restrict__ fin, long long i,
+                                              long long j, int k) {
+    const long long ni = i + DI(k), nj = j + DJ(k);
+    if (ni < 0 || nj < 0 || ni >= g.rows || nj >= g.cols) return 0.0;
+    const int b = opp(k);
+    return M::to_f64(M::load(fin + b * g.plane + nj * g.ld + ni), b);
+}
+
+template <class M>
+__global__ void __launch_bounds__(256) k_flow_forces(Geometry g, const typename M::T* __restrict__ fin,
+                                                     const int64_t* __restrict__ pts, const uint16_t* __restrict__ dirs,
+                                                     long long n, double2* partials) {
+    Neu acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+    constexpr double SQRT2 = 1.4142135623730951;  // sqrt(2) rounded to double
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        const long long i = pts[2 * q], j = pts[2 * q + 1];
+        const unsigned b = dirs[q];
+        double local_lift = 0., local_drag = 0.;
+        if (b & (1u << 1)) local_drag -= force_input<M>(g, fin, i, j, 1);
+        if (b & (1u << 2)) local_lift -= force_input<M>(g, fin, i, j, 2);
+        if (b & (1u << 3)) local_drag += force_input<M>(g, fin, i, j, 3);
+        if (b & (1u << 4)) local_lift += force_input<M>(g, fin, i, j, 4);
+        if (b & (1u << 5)) {
+            const double v = force_input<M>(g, fin, i, j, 5);
+            local_drag -= (v) * SQRT2 / 2.0;
+            local_lift -= (v) * SQRT2 / 2.0;
+        }
+        if (b & (1u << 6)) {
+            const double v = force_input<M>(g, fin, i, j, 6);
+            local_drag += (v) * SQRT2 / 2.0;
+            local_lift -= (v) * SQRT2 / 2.0;
+        }
+        if (b & (1u << 7)) {
+            const double v = force_input<M>(g, fin, i, j, 7);
+            local_drag += (v) * SQRT2 / 2.0;
+            local_lift += (v) * SQRT2 / 2.0;
+        }
+        if (b & (1u << 8)) {
+            const double v = force_input<M>(g, fin, i, j, 8);
+            local_drag -= (v) * SQRT2 / 2.0;
+            local_lift += (v) * SQRT2 / 2.0;
+        }
+        acc[0] = neu_add(acc[0], local_lift);
+        acc[1] = neu_add(acc[1], local_drag);
+    }
+    block_reduce_store<2>(acc, partials);
+}
+
+template <class M>
+__global__ void k_gather_forces(Geometry g, const typename M::T* __restrict__ fin, const int64_t* __restrict__ pts,
+                                const uint16_t* __restrict__ dirs, long long n, double* __restrict__ out) {
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const long long i = pts[2 * q], j = pts[2 * q + 1];
+    const unsigned b = dirs[q];
+#pragma unroll
+    for (int k = 1; k < 9; ++k) out[q * 8 + (k - 1)] = (b & (1u << k)) ? force_input<M>(g, fin, i, j, k) : 0.0;
+}
+
+}  // namespace llb

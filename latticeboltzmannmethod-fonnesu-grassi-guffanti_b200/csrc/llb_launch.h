@@ -1,0 +1,54 @@
+// Host-side launch interface between the C ABI (llb_capi.cu) and the
+// per-storage kernel translation units (llb_f64.cu, llb_lowp.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "llb_internal.cuh"
+
+namespace llb {
+
+struct LaunchCtx {
+    Geometry g;
+    OpenTable ot;
+    Collision c;
+    MacroOut mo;
+    StepSync ss;
+    cudaStream_t stream;
+};
+
+// Storage-specific entry points; `storage` is LLB_STORE_* and selects the
+// translation unit.  All launches go to ctx.stream and return the launch error.
+cudaError_t launch_step(int storage, const LaunchCtx& ctx, const void* fin, void* fout, bool init, bool macro);
+cudaError_t launch_finalize(int storage, const LaunchCtx& ctx, const void* fin, double* out, long long t);
+cudaError_t launch_export(int storage, const LaunchCtx& ctx, const void* fin, double* out);
+cudaError_t launch_mass_momentum(int storage, const LaunchCtx& ctx, const void* fin, double2* partials,
+                                 int nblocks, double* out3);
+cudaError_t launch_flow_forces(int storage, const LaunchCtx& ctx, const void* fin, const int64_t* pts,
+                               const uint16_t* dirs, long long n, double2* partials, int nblocks, double* out2);
+cudaError_t launch_gather_forces(int storage, const LaunchCtx& ctx, const void* fin, const int64_t* pts,
+                                 const uint16_t* dirs, long long n, double* out);
+
+// per translation unit
+cudaError_t launch_step_f64(const LaunchCtx&, const void*, void*, bool, bool);
+cudaError_t launch_finalize_f64(const LaunchCtx&, const void*, double*, long long);
+cudaError_t launch_export_f64(const LaunchCtx&, const void*, double*);
+cudaError_t launch_mass_momentum_f64(const LaunchCtx&, const void*, double2*, int, double*);
+cudaError_t launch_flow_forces_f64(const LaunchCtx&, const void*, const int64_t*, const uint16_t*, long long,
+                                   double2*, int, double*);
+cudaError_t launch_gather_forces_f64(const LaunchCtx&, const void*, const int64_t*, const uint16_t*, long long,
+                                     double*);
+cudaError_t launch_step_lowp(int storage, const LaunchCtx&, const void*, void*, bool, bool);
+cudaError_t launch_finalize_lowp(int storage, const LaunchCtx&, const void*, double*, long long);
+cudaError_t launch_export_lowp(int storage, const LaunchCtx&, const void*, double*);
+cudaError_t launch_mass_momentum_lowp(int storage, const LaunchCtx&, const void*, double2*, int, double*);
+cudaError_t launch_flow_forces_lowp(int storage, const LaunchCtx&, const void*, const int64_t*, const uint16_t*,
+                                    long long, double2*, int, double*);
+cudaError_t launch_gather_forces_lowp(int storage, const LaunchCtx&, const void*, const int64_t*,
+                                      const uint16_t*, long long, double*);
+
+inline dim3 node_grid(const Geometry& g, int bx, int by) {
+    return dim3(static_cast<unsigned>((g.rows + bx - 1) / bx), static_cast<unsigned>((g.cols + by - 1) / by));
+}
+
+}  // namespace llb

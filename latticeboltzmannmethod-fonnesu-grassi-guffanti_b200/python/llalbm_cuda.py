@@ -1,0 +1,284 @@
+"""ctypes binding of libllalbm_cuda.so (C ABI in include/llalbm_cuda.h).
+
+This is the Python face of the CUDA parallelization policy: a `CudaLattice`
+holds one lattice resident on a GPU and exposes the same operations the C++
+`CUDAPolicy` drives (init, steps, macroscopic output, populations, flow forces).
+Arrays use the reference's Eigen layouts; in numpy (C order) a populations
+tensor (R, C, 9) is `pop[k, j, i]`, u (R, C, 2) is `u[c, j, i]`, rho is `rho[j, i]`.
+
+The library is loaded from the package directory; a missing or unloadable
+library raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libllalbm_cuda.so")
+
+LLB_OK = 0
+ERRORS = {
+    -1: "LLB_E_INVALID", -2: "LLB_E_GEOMETRY", -3: "LLB_E_NOMEM", -4: "LLB_E_CUDA", -5: "LLB_E_NODEVICE",
+    -6: "LLB_E_STATE", -7: "LLB_E_NUMERIC", -8: "LLB_E_UNSUPPORTED", -9: "LLB_E_TIMEOUT",
+}
+BGK, TRT = 0, 1
+STORE_F64, STORE_F32S, STORE_F16S = 0, 1, 2
+PATTERN_AB, PATTERN_AA = 0, 1
+BC_ZH_VELOCITY, BC_OPEN, BC_ZH_PRESSURE = 0, 1, 2
+STEP_MACRO = 1
+STORAGE_BYTES = {STORE_F64: 8, STORE_F32S: 4, STORE_F16S: 2}
+
+
+class LLBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Desc(ctypes.Structure):
+    _fields_ = [
+        ("rows", ctypes.c_int64), ("cols", ctypes.c_int64),
+        ("n_fluid", ctypes.c_int64), ("fluid_ij", ctypes.c_void_p),
+        ("n_wall", ctypes.c_int64), ("wall_ij", ctypes.c_void_p),
+        ("n_inlet", ctypes.c_int64), ("inlet_ij", ctypes.c_void_p), ("inlet_side", ctypes.c_void_p),
+        ("n_outlet", ctypes.c_int64), ("outlet_ij", ctypes.c_void_p), ("outlet_side", ctypes.c_void_p),
+        ("n_obstacle", ctypes.c_int64), ("obstacle_ij", ctypes.c_void_p), ("obstacle_dirs", ctypes.c_void_p),
+        ("inlet_bc", ctypes.c_int32), ("outlet_bc", ctypes.c_int32),
+        ("collision", ctypes.c_int32), ("tau", ctypes.c_double),
+        ("tau_even", ctypes.c_double), ("tau_odd", ctypes.c_double),
+        ("storage", ctypes.c_int32), ("pattern", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("open_table_rows", ctypes.c_int32),
+    ]
+
+
+class _NodeLists(ctypes.Structure):
+    _fields_ = [
+        ("n_fluid", ctypes.c_int64), ("n_wall", ctypes.c_int64), ("n_inlet", ctypes.c_int64),
+        ("n_outlet", ctypes.c_int64), ("n_obstacle", ctypes.c_int64),
+        ("fluid_ij", ctypes.c_void_p), ("wall_ij", ctypes.c_void_p),
+        ("inlet_ij", ctypes.c_void_p), ("inlet_side", ctypes.c_void_p),
+        ("outlet_ij", ctypes.c_void_p), ("outlet_side", ctypes.c_void_p),
+        ("obstacle_ij", ctypes.c_void_p), ("obstacle_dirs", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+# every exported function: (name, argtypes)
+_H = ctypes.c_void_p
+_P = ctypes.c_void_p
+SIGNATURES = {
+    "llb_abi_version": [],
+    "llb_last_error": [_H],
+    "llb_classify_count": [ctypes.c_int64, ctypes.c_int64, _P, _P],
+    "llb_classify_fill": [ctypes.c_int64, ctypes.c_int64, _P, ctypes.POINTER(_NodeLists)],
+    "llb_create": [ctypes.POINTER(_Desc), ctypes.POINTER(_H)],
+    "llb_destroy": [_H],
+    "llb_set_open_values": [_H, ctypes.c_int64, ctypes.c_int32, _P],
+    "llb_init": [_H, ctypes.c_uint32],
+    "llb_step": [_H, ctypes.c_int32, ctypes.c_uint32],
+    "llb_get_step": [_H, ctypes.POINTER(ctypes.c_int64)],
+    "llb_get_macro": [_H, _P, _P],
+    "llb_get_populations": [_H, _P],
+    "llb_get_post_collision": [_H, _P],
+    "llb_set_force_points": [_H, _P, _P, ctypes.c_int64],
+    "llb_flow_forces": [_H, _P],
+    "llb_gather_force_inputs": [_H, _P],
+    "llb_mass_momentum": [_H, _P],
+    "llb_synchronize": [_H],
+    "llb_check_numerics": [_H],
+    "llb_event_record": [_H, ctypes.c_int32],
+    "llb_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
+    "llb_device_bytes": [_H, ctypes.POINTER(ctypes.c_int64)],
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the in-tree library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with build.py (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_char_p if name == "llb_last_error" else ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, h=None):
+    if rc != LLB_OK:
+        msg = lib().llb_last_error(h)
+        raise LLBError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None and a.size else None
+
+
+def _ij(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64).reshape(-1, 2))
+
+
+def classify(types: np.ndarray) -> dict:
+    """Reference node vectors from an (R, C) grid of InputNodeType codes
+    (read_lattice_file's classification, in O(R*C))."""
+    R, C = types.shape
+    grid = np.ascontiguousarray(np.asarray(types, dtype=np.uint8).T)  # column-major (i fastest)
+    counts = np.zeros(5, dtype=np.int64)
+    _check(lib().llb_classify_count(R, C, _ptr(grid), _ptr(counts)))
+    nf, nw, ni, no, nb = (int(c) for c in counts)
+    out = {
+        "fluid": np.zeros((nf, 2), np.int64), "wall": np.zeros((nw, 2), np.int64),
+        "inlet": np.zeros((ni, 2), np.int64), "inlet_side": np.zeros(ni, np.int32),
+        "outlet": np.zeros((no, 2), np.int64), "outlet_side": np.zeros(no, np.int32),
+        "obstacle": np.zeros((nb, 2), np.int64), "obstacle_dirs": np.zeros(nb, np.uint16),
+    }
+    nl = _NodeLists(nf, nw, ni, no, nb, _ptr(out["fluid"]), _ptr(out["wall"]), _ptr(out["inlet"]),
+                    _ptr(out["inlet_side"]), _ptr(out["outlet"]), _ptr(out["outlet_side"]),
+                    _ptr(out["obstacle"]), _ptr(out["obstacle_dirs"]))
+    _check(lib().llb_classify_fill(R, C, _ptr(grid), ctypes.byref(nl)))
+    return out
+
+
+class CudaLattice:
+    """One D2Q9 lattice resident on a GPU (the engine behind CUDAPolicy)."""
+
+    def __init__(self, rows: int, cols: int, fluid, wall, inlet, inlet_side, outlet, outlet_side,
+                 obstacle, obstacle_dirs=None, *, collision: int = BGK, tau: float = 0.6,
+                 tau_even: float = 0.6, tau_odd: float = 0.6, inlet_bc: int = BC_ZH_VELOCITY,
+                 outlet_bc: int = BC_ZH_VELOCITY, storage: int = STORE_F64, pattern: int = PATTERN_AB,
+                 device: int = 0, open_table_rows: int = 1):
+        self.rows, self.cols = int(rows), int(cols)
+        self.storage = storage
+        keep = {
+            "fluid": _ij(fluid), "wall": _ij(wall), "inlet": _ij(inlet), "outlet": _ij(outlet),
+            "obstacle": _ij(obstacle),
+            "inlet_side": np.ascontiguousarray(np.asarray(inlet_side, dtype=np.int32).reshape(-1)),
+            "outlet_side": np.ascontiguousarray(np.asarray(outlet_side, dtype=np.int32).reshape(-1)),
+        }
+        keep["obstacle_dirs"] = (None if obstacle_dirs is None else
+                                 np.ascontiguousarray(np.asarray(obstacle_dirs, dtype=np.uint16).reshape(-1)))
+        self.n_inlet, self.n_outlet = len(keep["inlet"]), len(keep["outlet"])
+        self.n_open = self.n_inlet + self.n_outlet
+        self.n_active = len(keep["fluid"]) + self.n_open
+        d = _Desc(self.rows, self.cols,
+                  len(keep["fluid"]), _ptr(keep["fluid"]), len(keep["wall"]), _ptr(keep["wall"]),
+                  self.n_inlet, _ptr(keep["inlet"]), _ptr(keep["inlet_side"]),
+                  self.n_outlet, _ptr(keep["outlet"]), _ptr(keep["outlet_side"]),
+                  len(keep["obstacle"]), _ptr(keep["obstacle"]), _ptr(keep["obstacle_dirs"]),
+                  inlet_bc, outlet_bc, collision, tau, tau_even, tau_odd, storage, pattern, device,
+                  open_table_rows)
+        h = ctypes.c_void_p()
+        _check(lib().llb_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self._force_n = 0
+
+    # -- lifetime --------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().llb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- stepping ----------------------------------------------------------------
+    def set_open_values(self, values: np.ndarray, t_first: int = 0):
+        """values: [rows][n_open][2] boundary values for steps t_first.. (inlets first)."""
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1, self.n_open, 2)
+        _check(lib().llb_set_open_values(self._h, t_first, v.shape[0], _ptr(v)), self._h)
+
+    def init(self, macro: bool = False):
+        _check(lib().llb_init(self._h, STEP_MACRO if macro else 0), self._h)
+
+    def step(self, n: int = 1, macro: bool = False):
+        _check(lib().llb_step(self._h, n, STEP_MACRO if macro else 0), self._h)
+
+    @property
+    def t(self) -> int:
+        s = ctypes.c_int64()
+        _check(lib().llb_get_step(self._h, ctypes.byref(s)), self._h)
+        return s.value
+
+    def synchronize(self):
+        _check(lib().llb_synchronize(self._h), self._h)
+
+    def check_numerics(self):
+        _check(lib().llb_check_numerics(self._h), self._h)
+
+    # -- results -----------------------------------------------------------------
+    def macro(self):
+        rho = np.empty((self.cols, self.rows)); u = np.empty((2, self.cols, self.rows))
+        _check(lib().llb_get_macro(self._h, _ptr(rho), _ptr(u)), self._h)
+        return rho, u
+
+    def populations(self) -> np.ndarray:
+        out = np.empty((9, self.cols, self.rows))
+        _check(lib().llb_get_populations(self._h, _ptr(out)), self._h)
+        return out
+
+    def post_collision(self) -> np.ndarray:
+        out = np.empty((9, self.cols, self.rows))
+        _check(lib().llb_get_post_collision(self._h, _ptr(out)), self._h)
+        return out
+
+    def set_force_points(self, pts, dirs):
+        p = _ij(pts); q = np.ascontiguousarray(np.asarray(dirs, dtype=np.uint16).reshape(-1))
+        _check(lib().llb_set_force_points(self._h, _ptr(p), _ptr(q), len(p)), self._h)
+        self._force_n = len(p)
+
+    def flow_forces(self):
+        out = np.zeros(2)
+        _check(lib().llb_flow_forces(self._h, _ptr(out)), self._h)
+        return float(out[0]), float(out[1])
+
+    def gather_force_inputs(self) -> np.ndarray:
+        out = np.zeros((self._force_n, 8))
+        _check(lib().llb_gather_force_inputs(self._h, _ptr(out)), self._h)
+        return out
+
+    def mass_momentum(self) -> np.ndarray:
+        out = np.zeros(3)
+        _check(lib().llb_mass_momentum(self._h, _ptr(out)), self._h)
+        return out
+
+    # -- timing --------------------------------------------------------------------
+    def record(self, slot: int):
+        _check(lib().llb_event_record(self._h, slot), self._h)
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = ctypes.c_float()
+        _check(lib().llb_event_elapsed_ms(self._h, a, b, ctypes.byref(ms)), self._h)
+        return float(ms.value)
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64()
+        _check(lib().llb_device_bytes(self._h, ctypes.byref(b)), self._h)
+        return b.value
+
+
+def from_types(types: np.ndarray, **kw) -> CudaLattice:
+    """CudaLattice from an (R, C) InputNodeType grid, classified like the reference."""
+    n = classify(types)
+    R, C = types.shape
+    return CudaLattice(R, C, n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"], n["outlet_side"],
+                       n["obstacle"], n["obstacle_dirs"], **kw)

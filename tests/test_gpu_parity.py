@@ -1,0 +1,198 @@
+"""Parity of the CUDA path (through the C ABI) with the C oracle.
+
+The FP64 path must equal the oracle bit for bit on populations of fluid, inlet
+and outlet nodes, on u and rho, and on the post-collision state; the oracle is
+itself pinned bit for bit to the reference (tests/test_oracle.py).
+"""
+import numpy as np
+import pytest
+
+import harness as H
+
+pytestmark = pytest.mark.gpu
+
+
+def make_gpu(lists: H.NodeLists, p: H.Params, storage=0, table_rows=1):
+    import llalbm_cuda as L
+
+    return L.CudaLattice(lists.rows, lists.cols, lists.fluid, lists.wall, lists.inlet, lists.inlet_side,
+                         lists.outlet, lists.outlet_side, lists.obstacle, lists.obstacle_dirs,
+                         collision=p.collision, tau=p.tau, tau_even=p.tau_even, tau_odd=p.tau_odd,
+                         inlet_bc=p.inlet_bc, outlet_bc=p.outlet_bc, storage=storage,
+                         open_table_rows=table_rows)
+
+
+def pressure_table(table: np.ndarray, lists: H.NodeLists, p: H.Params) -> np.ndarray:
+    """Pressure-policy nodes take (rho0, tangential u) instead of a velocity."""
+    t = table.copy()
+    if p.inlet_bc == H.BC_ZH_PRESSURE:
+        t[:, : len(lists.inlet)] = (p.rho_out, p.tangential_u)
+    if p.outlet_bc == H.BC_ZH_PRESSURE:
+        t[:, len(lists.inlet):] = (p.rho_out, p.tangential_u)
+    return t
+
+
+def run_gpu(lists, p, steps, table, storage=0):
+    tab = pressure_table(table, lists, p)
+    rows = tab.shape[0]
+    with make_gpu(lists, p, storage=storage, table_rows=max(rows, 1)) as g:
+        if lists.n_open:
+            g.set_open_values(tab, 0)
+        g.init(macro=(steps == 1))
+        if steps > 1:
+            g.step(steps - 1, macro=True)
+        pop = g.populations()
+        rho, u = g.macro()
+        post = g.post_collision()
+        g.check_numerics()
+        return {"populations": pop, "rho": rho, "u": u, "post": post, "t": g.t}
+
+
+def cases():
+    cav = H.classify(H.cavity_types(129))
+    yield "cavity129_bgk", cav, H.Params(tau=0.884), "const:0.1:0", "const:0:0"
+    cav64 = H.classify(H.cavity_types(64))
+    yield "cavity64_trt_ramp", cav64, H.Params.trt_magic(0.58), "lidramp:0.15:0.001", "const:0:0"
+    ch = H.classify(H.channel_types(48, 96, discs=[(24, 30, 6), (12, 60, 4)]))
+    yield ("channel_trt_parabolic_pressure", ch,
+           H.Params.trt_magic(0.53, outlet_bc=H.BC_ZH_PRESSURE), "parabolic:0.05:1:46", "pressure")
+    ch2 = H.classify(H.channel_types(40, 80, discs=[(20, 25, 5)]))
+    yield "channel_bgk_open_outlet", ch2, H.Params(tau=0.7, outlet_bc=H.BC_OPEN), "const:0.04:0", "const:0:0"
+    yield "channel_trt_zh_outlet", ch2, H.Params.trt_magic(0.7), "const:0.04:0", "const:0.04:0"
+    odd = H.channel_types(37, 53, discs=[(18, 20, 4)])
+    odd[1:-1, 0] = H.BOUNDARY
+    odd[:, 0] = H.INLET               # inlet column including both corner nodes (no closure there)
+    odd[20, 30] = H.SOLID             # file-SOLID node next to fluid: its sources keep their initial value
+    yield "odd_corners_solid", H.classify(odd), H.Params(tau=0.8), "const:0.03:0.01", "const:0:0"
+    pres_in = H.classify(H.channel_types(30, 60, discs=[(15, 20, 4)]))
+    yield ("pressure_inlet_velocity_outlet", pres_in, H.Params(tau=0.9, inlet_bc=H.BC_ZH_PRESSURE,
+           rho_out=1.01), "pressure", "const:0.02:0")
+
+
+CASES = list(cases())
+
+
+@pytest.mark.parametrize("steps", [1, 2, 7, 100, 1000])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_f64_bit_exact(case, steps):
+    name, lists, p, ins, outs = case
+    table = H.open_values(lists, ins, outs, steps)
+    ref = H.run_oracle(lists, p, steps, table)
+    got = run_gpu(lists, p, steps, table)
+    act = H.active_mask(lists)
+    assert got["t"] == steps
+    np.testing.assert_array_equal(got["populations"][:, act], ref["populations"][:, act])
+    np.testing.assert_array_equal(got["post"][:, act], ref["post"][:, act])
+    np.testing.assert_array_equal(got["u"], ref["u"])
+    np.testing.assert_array_equal(got["rho"], ref["rho"])
+
+
+def test_cavity129_10k_steps_bit_exact():
+    """Config 1 (129x129 lid cavity, BGK tau 0.884, lid u = (0.1, 0)) after 10 000 steps."""
+    lists = H.classify(H.cavity_types(129))
+    p = H.Params(tau=0.884)
+    table = H.open_values(lists, "const:0.1:0", "const:0:0", 1)
+    ref = H.run_oracle(lists, p, 10000, table)
+    got = run_gpu(lists, p, 10000, table)
+    act = H.active_mask(lists)
+    diff = np.abs(got["populations"][:, act] - ref["populations"][:, act]).max()
+    assert diff <= 1e-12
+    np.testing.assert_array_equal(got["populations"][:, act], ref["populations"][:, act])
+    np.testing.assert_array_equal(got["u"], ref["u"])
+
+
+def rel_l2(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+@pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3)], ids=["f32s", "f16s"])
+def test_shifted_storage_velocity_error(storage, tol):
+    lists = H.classify(H.channel_types(64, 160, discs=[(32, 40, 8)]))
+    p = H.Params.trt_magic(0.56, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "parabolic:0.05:1:62", "pressure", 1)
+    steps = 2000
+    ref = H.run_oracle(lists, p, steps, table)
+    got = run_gpu(lists, p, steps, table, storage=storage)
+    err = rel_l2(got["u"], ref["u"])
+    assert err <= tol, err
+
+
+def test_flow_forces_and_gather():
+    lists = H.classify(H.channel_types(48, 96, discs=[(24, 30, 6)]))
+    p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "parabolic:0.05:1:46", "pressure", 1)
+    steps = 300
+    ref = H.run_oracle(lists, p, steps, table)
+    lift_ref, drag_ref = H.oracle_flow_properties(lists.rows, lists.cols, ref["post"], lists.obstacle,
+                                                  lists.obstacle_dirs)
+    with make_gpu(lists, p) as g:
+        g.set_open_values(pressure_table(table, lists, p))
+        g.init()
+        g.step(steps - 1)
+        g.set_force_points(lists.obstacle, lists.obstacle_dirs)
+        lift, drag = g.flow_forces()
+        vals = g.gather_force_inputs()
+        post = g.post_collision()
+    assert abs(lift - lift_ref) <= 1e-12 * max(1.0, abs(lift_ref))
+    assert abs(drag - drag_ref) <= 1e-12 * max(1.0, abs(drag_ref))
+    # gathered inputs are exactly the post-collision values the analyzer reads
+    opp = [0, 3, 4, 1, 2, 7, 8, 5, 6]
+    for q, ((i, j), b) in enumerate(zip(lists.obstacle, lists.obstacle_dirs)):
+        for k in range(1, 9):
+            want = ref["post"][opp[k], j + H.DJ[k], i + H.DI[k]] if (int(b) >> k) & 1 else 0.0
+            assert vals[q, k - 1] == want
+    np.testing.assert_array_equal(post[:, H.active_mask(lists)], ref["post"][:, H.active_mask(lists)])
+
+
+def test_mass_momentum_compensated():
+    lists = H.classify(H.cavity_types(96))
+    p = H.Params(tau=0.7)
+    table = H.open_values(lists, "const:0.08:0", "const:0:0", 1)
+    ref = H.run_oracle(lists, p, 500, table)
+    with make_gpu(lists, p) as g:
+        g.set_open_values(table)
+        g.init()
+        g.step(499)
+        mm = g.mass_momentum()
+    act = H.active_mask(lists)
+    f = ref["post"][:, act]
+    import math
+    mass = math.fsum(f.sum(axis=0).tolist())
+    mx = math.fsum(((f[1] + f[5] + f[8]) - (f[3] + f[6] + f[7])).tolist())
+    my = math.fsum(((f[2] + f[5] + f[6]) - (f[4] + f[7] + f[8])).tolist())
+    assert abs(mm[0] - mass) <= 1e-12 * abs(mass)
+    assert abs(mm[1] - mx) <= 1e-12 * max(1.0, abs(mx))
+    assert abs(mm[2] - my) <= 1e-12 * max(1.0, abs(my))
+
+
+def test_graph_replay_matches_single_launches():
+    """Multi-step calls replay CUDA graphs; results must not depend on the chunking."""
+    lists = H.classify(H.channel_types(40, 80, discs=[(20, 25, 5)]))
+    p = H.Params(tau=0.7, outlet_bc=H.BC_OPEN)
+    table = H.open_values(lists, "const:0.04:0", "const:0:0", 1)
+    outs = []
+    for chunks in ([199], [1] * 199, [31, 64, 33, 71]):
+        with make_gpu(lists, p) as g:
+            g.set_open_values(table)
+            g.init()
+            for c in chunks:
+                g.step(c)
+            outs.append(g.populations())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
+
+
+def test_numerics_flag():
+    """An unstable run (tau near 0.5, strong lid) is reported as LLB_E_NUMERIC."""
+    import llalbm_cuda as L
+
+    lists = H.classify(H.cavity_types(32))
+    p = H.Params(tau=0.5001)
+    table = H.open_values(lists, "const:0.6:0", "const:0:0", 1)
+    with make_gpu(lists, p) as g:
+        g.set_open_values(table)
+        g.init()
+        g.step(5000)
+        with pytest.raises(L.LLBError) as e:
+            g.check_numerics()
+        assert e.value.code == -7
