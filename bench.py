@@ -48,11 +48,12 @@ REF_FAST = os.path.join(ROOT, "oracle", "_ref", "ref_runner_fast")
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def workload(name: str) -> dict:
+def workload(name: str, size: int = 4096) -> dict:
     if name == "porous4096":
-        return dict(name=name, desc="random porous channel 4096x4096, 30% solid discs r 3..12, BGK tau 0.8, "
+        return dict(name=name if size == 4096 else f"porous{size}",
+                    desc=f"random porous channel {size}x{size}, 30% solid discs r 3..12, BGK tau 0.8, "
                     "Zou-He velocity inlet u=0.02, Zou-He pressure outlet rho=1",
-                    types=lambda: W.porous_types(4096, 4096), collision=0, tau=0.8, tau_even=0.8, tau_odd=0.8,
+                    types=lambda: W.porous_types(size, size), collision=0, tau=0.8, tau_even=0.8, tau_odd=0.8,
                     inlet=("const", 0.02, 0.0), outlet_bc=2, rho_out=1.0, ref_args=[
                         "--collision", "bgk", "--tau", "0.8", "--inlet", "zh", "--outlet", "zhp",
                         "--inlet-u", "const:0.02:0", "--outlet-u", "pressure"])
@@ -268,7 +269,7 @@ def time_form(L, wl, nodes, R, C, storage, device, warmup, steps, dist, sampler=
 def run_ours(a, dist):
     import llalbm_cuda as L
 
-    wl = workload(a.workload)
+    wl = workload(a.workload, a.size)
     types = wl["types"]()
     R, C = types.shape
     nodes = L.classify(types)
@@ -279,6 +280,8 @@ def run_ours(a, dist):
     u_ref = None
     head = None
     for storage, name, sb in ((0, "f64", 8), (1, "f32s", 4), (2, "f16s", 2)):
+        if name not in a.forms.split(","):
+            continue
         g, ms, (t0, t1), u = time_form(L, wl, nodes, R, C, storage, dev, a.warmup, a.steps, dist)
         per = ms / a.steps
         bps = bytes_per_step(sb, n_active, R * C)
@@ -362,6 +365,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="porous4096", choices=("porous4096", "cylinder1024x256", "cavity129"))
+    ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous workload")
+    ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
@@ -370,7 +375,7 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return
-        wl = workload(a.workload)
+        wl = workload(a.workload, a.size)
         types = wl["types"]()
         w, k = min(a.warmup, 2), max(1, min(a.steps, 5 if a.workload == "porous4096" else 200))
         r = reference_cpu(wl, types, w, k)

@@ -186,6 +186,9 @@ int llb_check_numerics(llb_handle h);
 /* CUDA events on the handle's stream: slot in [0, 8). */
 int llb_event_record(llb_handle h, int32_t slot);
 int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, float* ms);
+/* Columns of lattice nodes per thread block of the step kernel (1..8; each
+   block is 32 rows x block_y columns).  A tuning knob for the autotuner. */
+int llb_set_launch_shape(llb_handle h, int32_t block_y);
 /* Device bytes held by the handle. */
 int llb_device_bytes(llb_handle h, int64_t* bytes);
 /* Message for the last error on this handle (or the last global error for NULL). */

@@ -42,9 +42,9 @@ struct llb_lattice {
     double* d_rho = nullptr;
     double* d_u = nullptr;
     double* d_dense = nullptr;
-    long long* d_step = nullptr;
-    unsigned* d_done = nullptr;
+    long long* d_step = nullptr;  // step index at the start of a graph replay
     unsigned* d_flags = nullptr;
+    int block_y = 4;
     double2* d_partials = nullptr;
     int partial_blocks = 0;
     double* d_red = nullptr;
@@ -109,10 +109,11 @@ LaunchCtx make_ctx(llb_handle h) {
     x.c = h->coll;
     x.mo.rho = h->d_rho;
     x.mo.u = h->d_u;
-    x.ss.step = h->d_step;
-    x.ss.done = h->d_done;
+    x.ss.tbase = nullptr;
+    x.ss.t_off = h->step;
     x.ss.flags = h->d_flags;
     x.stream = h->stream;
+    x.block_y = h->block_y;
     return x;
 }
 
@@ -123,7 +124,7 @@ void release(llb_handle h) {
     for (auto& g : h->graph)
         if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
-                    h->d_step, h->d_done, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
+                    h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (auto& e : h->ev)
@@ -226,8 +227,14 @@ int ensure_partials(llb_handle h, int nblocks) {
     return LLB_OK;
 }
 
-int launch_one(llb_handle h, bool macro) {
+// One step kernel.  Inside a graph capture the step index is relative
+// (graph_offset >= 0, base read from d_step); otherwise it is absolute.
+int launch_one(llb_handle h, bool macro, long long graph_offset = -1) {
     LaunchCtx x = make_ctx(h);
+    if (graph_offset >= 0) {
+        x.ss.tbase = h->d_step;
+        x.ss.t_off = graph_offset;
+    }
     cudaError_t e = launch_step(h->storage, x, h->f[h->cur], h->f[h->cur ^ 1], false, macro);
     if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
     h->cur ^= 1;
@@ -242,7 +249,7 @@ int graph_for(llb_handle h, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     LLB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int rc = LLB_OK;
-    for (int s = 0; s < GRAPH_STEPS && rc == LLB_OK; ++s) rc = launch_one(h, false);
+    for (int s = 0; s < GRAPH_STEPS && rc == LLB_OK; ++s) rc = launch_one(h, false, s);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->cur = cur0;
     h->step = step0;
@@ -359,8 +366,7 @@ int llb_create(const llb_desc* d, llb_handle* out) {
         (rc = dev_alloc(h, &h->d_open_idx, open_idx.size() * sizeof(int32_t))) ||
         (rc = dev_alloc(h, &h->d_open, sizeof(double2) * static_cast<size_t>(std::max<int64_t>(n_open, 1)) * cap)) ||
         (rc = dev_alloc(h, &h->d_rho, sizeof(double) * N)) || (rc = dev_alloc(h, &h->d_u, sizeof(double) * 2 * N)) ||
-        (rc = dev_alloc(h, &h->d_step, sizeof(long long))) || (rc = dev_alloc(h, &h->d_done, sizeof(unsigned))) ||
-        (rc = dev_alloc(h, &h->d_flags, sizeof(unsigned))) || (rc = dev_alloc(h, &h->d_red, sizeof(double) * 4)))
+        (rc = dev_alloc(h, &h->d_step, sizeof(long long))) || (rc = dev_alloc(h, &h->d_flags, sizeof(unsigned))) || (rc = dev_alloc(h, &h->d_red, sizeof(double) * 4)))
         return bail(rc);
     e = cudaMemcpyAsync(h->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)
@@ -369,7 +375,6 @@ int llb_create(const llb_desc* d, llb_handle* out) {
         e = cudaMemsetAsync(h->d_open, 0, sizeof(double2) * static_cast<size_t>(std::max<int64_t>(n_open, 1)) * cap, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->f[0], 0, pop_bytes, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->f[1], 0, pop_bytes, h->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_done, 0, sizeof(unsigned), h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "lattice upload"));
@@ -407,9 +412,8 @@ int llb_init(llb_handle h, uint32_t flags) {
     if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
     int rc = select_device(h);
     if (rc) return rc;
-    LLB_CUDA(h, cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream));
-    LLB_CUDA(h, cudaMemsetAsync(h->d_done, 0, sizeof(unsigned), h->stream));
     h->cur = 0;
+    h->step = 0;
     LaunchCtx x = make_ctx(h);
     const bool macro = (flags & LLB_STEP_MACRO) != 0;
     cudaError_t e = launch_step(h->storage, x, nullptr, h->f[0], true, macro);
@@ -432,6 +436,8 @@ int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
         cudaGraphExec_t g = nullptr;
         if ((rc = graph_for(h, &g))) return rc;
         while (plain >= GRAPH_STEPS) {
+            // the replay's step base; a pageable source is staged at call time
+            LLB_CUDA(h, cudaMemcpyAsync(h->d_step, &h->step, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
             LLB_CUDA(h, cudaGraphLaunch(g, h->stream));
             h->step += GRAPH_STEPS;
             plain -= GRAPH_STEPS;
@@ -588,6 +594,19 @@ int llb_event_elapsed_ms(llb_handle h, int32_t a, int32_t b, float* ms) {
     if (rc) return rc;
     LLB_CUDA(h, cudaEventSynchronize(h->ev[b]));
     LLB_CUDA(h, cudaEventElapsedTime(ms, h->ev[a], h->ev[b]));
+    return LLB_OK;
+}
+
+int llb_set_launch_shape(llb_handle h, int32_t block_y) {
+    if (!h || block_y < 1 || block_y > MAX_BLOCK_Y) return fail(h, LLB_E_INVALID, "block_y must be in [1, 8]");
+    if (block_y != h->block_y) {
+        int rc = select_device(h);
+        if (rc) return rc;
+        LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (auto& g : h->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        h->block_y = block_y;
+    }
     return LLB_OK;
 }
 

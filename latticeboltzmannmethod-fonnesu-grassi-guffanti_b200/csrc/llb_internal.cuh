@@ -64,6 +64,8 @@ __host__ __device__ constexpr double w_init(int k) {
 __host__ __device__ constexpr float w_f32(int k) { return k == 0 ? 4.0f / 9.0f : (k <= 4 ? 1.0f / 9.0f : 1.0f / 36.0f); }
 
 // ---- kernel parameters ------------------------------------------------------
+constexpr int MAX_BLOCK_Y = 8;  // columns per block of the step kernel, at most
+
 struct Geometry {
     int rows, cols;     // R, C
     int ld;             // column stride (elements) of populations / mask / open_idx
@@ -91,9 +93,12 @@ struct MacroOut {
     double* u;          // (R, C, 2) dense
 };
 
+// Step index of a launch: t = (tbase ? *tbase : 0) + t_off.  Direct launches
+// pass the absolute step in t_off; graph replays pass the step's offset inside
+// the graph and the host sets *tbase before each replay.
 struct StepSync {
-    long long* step;    // device step counter (index of the step being computed)
-    unsigned* done;     // blocks finished in the current launch
+    const long long* tbase;
+    long long t_off;
     unsigned* flags;    // bit 0: non-finite density seen
 };
 

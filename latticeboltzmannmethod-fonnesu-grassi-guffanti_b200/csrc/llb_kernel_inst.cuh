@@ -9,7 +9,8 @@ namespace llb {
 template <class M>
 cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
     using T = typename M::T;
-    const dim3 block(BX, BY), grid = node_grid(x.g, BX, BY);
+    const int by = x.block_y >= 1 && x.block_y <= BY ? x.block_y : BY;
+    const dim3 block(BX, by), grid = node_grid(x.g, BX, by);
     const T* in = static_cast<const T*>(fin);
     T* out = static_cast<T*>(fout);
 #define LLB_STEP(COLL, MAC, INI) k_step<M, COLL, MAC, INI><<<grid, block, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss)

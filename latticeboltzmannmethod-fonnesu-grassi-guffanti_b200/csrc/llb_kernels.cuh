@@ -22,7 +22,7 @@
 
 namespace llb {
 
-constexpr int BX = 32, BY = 8;
+constexpr int BX = 32, BY = MAX_BLOCK_Y;  // one warp = 32 rows of one column
 
 template <class M>
 __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __restrict__ fin, int i, int j,
@@ -75,35 +75,44 @@ __device__ __forceinline__ void open_node(const OpenTable& ot, int q, uint8_t m,
     }
 }
 
-__device__ __forceinline__ void finish_block(const StepSync& ss, long long t, bool bad) {
-    const unsigned full = 0xffffffffu;
-    if (__any_sync(full, bad) && (threadIdx.x & 31) == 0) atomicOr(ss.flags, 1u);
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        __threadfence();
-        const unsigned total = gridDim.x * gridDim.y;
-        const unsigned prev = atomicAdd(ss.done, 1u);
-        if (prev == total - 1) {
-            *ss.done = 0u;
-            *ss.step = t + 1;
-            __threadfence();
-        }
-    }
+__device__ __forceinline__ long long current_step(const StepSync& ss) {
+    return (ss.tbase ? *ss.tbase : 0LL) + ss.t_off;
+}
+
+// Non-finite densities raise bit 0 of the flag word (one atomic per warp that
+// saw one).  No block-wide barrier: warps of a block finish independently.
+__device__ __forceinline__ void flag_numerics(const StepSync& ss, bool bad) {
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(ss.flags, 1u);
+}
+
+// Stores of a warp cover whole 32-byte sectors when every lane of a sector
+// writes: lanes of inactive nodes that share a sector with an active node
+// store too (their value is never read), so L2 never has to merge a partial
+// sector with DRAM contents.  Lanes whose whole sector is inactive skip.
+template <class M>
+__device__ __forceinline__ bool sector_has_active(bool active) {
+    constexpr int lanes_per_sector = 32 / sizeof(typename M::T);
+    const unsigned ballot = __ballot_sync(0xffffffffu, active);
+    const int lane = threadIdx.x & 31;
+    const unsigned group = ((1u << lanes_per_sector) - 1u) << (lane & ~(lanes_per_sector - 1));
+    return (ballot & group) != 0u;
 }
 
 // INIT == true: step 0 from the initial equilibrium (Lattice.hpp:326-328).
+// Block: 32 rows (one warp per column) x blockDim.y columns, blockDim.y <= BY.
 template <class M, int COLL, bool MACRO, bool INIT>
 __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Collision c,
                                                  const typename M::T* __restrict__ fin,
                                                  typename M::T* __restrict__ fout, MacroOut mo, StepSync ss) {
-    const long long t = INIT ? 0 : *reinterpret_cast<volatile long long*>(ss.step);
     const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     bool bad = false;
-    if (i < g.rows && j < g.cols) {
-        const long long node = static_cast<long long>(j) * g.ld + i;
-        const uint8_t m = g.mask[node];
-        const uint8_t cls = mask_class(m);
+    const bool inside = i < g.rows && j < g.cols;
+    const long long node = static_cast<long long>(j) * g.ld + i;
+    const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
+    const uint8_t cls = mask_class(m);
+    const bool write_sector = sector_has_active<M>(class_active(cls));
+    if (inside) {
         if (class_active(cls)) {
             typename M::R f[9];
             if (INIT) {
@@ -115,6 +124,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
             double rho, ux, uy;
             typename M::R rr;
             if (cls == CLS_OPEN) {
+                const long long t = INIT ? 0 : current_step(ss);
                 open_node<M>(ot, g.open_idx[node], m, t, f, rho, ux, uy);
                 rr = M::from_f64(rho);
             } else {
@@ -136,15 +146,25 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
             M::template collide<COLL>(f, rr, ux, uy, c);
 #pragma unroll
             for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
-        } else if (MACRO) {
-            const long long d = static_cast<long long>(j) * g.rows + i;
-            const long long N = static_cast<long long>(g.rows) * g.cols;
-            mo.rho[d] = 1.0;  // global_rho / global_u keep their initial values off active nodes
-            mo.u[d] = 0.0;
-            mo.u[d + N] = 0.0;
+        } else {
+            if (write_sector) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, typename M::R(0));
+            }
+            if (MACRO) {
+                const long long d = static_cast<long long>(j) * g.rows + i;
+                const long long N = static_cast<long long>(g.rows) * g.cols;
+                mo.rho[d] = 1.0;  // global_rho / global_u keep their initial values off active nodes
+                mo.u[d] = 0.0;
+                mo.u[d + N] = 0.0;
+            }
         }
+    } else if (write_sector && j < g.cols && i < g.ld) {
+        // padding rows of a column that shares a sector with active nodes
+#pragma unroll
+        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, typename M::R(0));
     }
-    finish_block(ss, t, bad);
+    flag_numerics(ss, bad);
 }
 
 // populations S_t = stream + bounce-back + closures of the resident state,

@@ -15,6 +15,7 @@ struct LaunchCtx {
     MacroOut mo;
     StepSync ss;
     cudaStream_t stream;
+    int block_y;        // columns per block of the step kernel (1..8)
 };
 
 // Storage-specific entry points; `storage` is LLB_STORE_* and selects the

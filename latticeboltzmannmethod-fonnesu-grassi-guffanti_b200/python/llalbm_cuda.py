@@ -92,6 +92,7 @@ SIGNATURES = {
     "llb_check_numerics": [_H],
     "llb_event_record": [_H, ctypes.c_int32],
     "llb_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
+    "llb_set_launch_shape": [_H, ctypes.c_int32],
     "llb_device_bytes": [_H, ctypes.POINTER(ctypes.c_int64)],
 }
 
@@ -269,6 +270,9 @@ class CudaLattice:
         ms = ctypes.c_float()
         _check(lib().llb_event_elapsed_ms(self._h, a, b, ctypes.byref(ms)), self._h)
         return float(ms.value)
+
+    def set_launch_shape(self, block_y: int):
+        _check(lib().llb_set_launch_shape(self._h, block_y), self._h)
 
     def device_bytes(self) -> int:
         b = ctypes.c_int64()
