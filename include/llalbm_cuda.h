@@ -181,13 +181,20 @@ int llb_mass_momentum(llb_handle h, double out[3]);
 
 int llb_synchronize(llb_handle h);
 /* LLB_E_NUMERIC if any step since the last call produced a non-finite density
-   (the reference's LLALBM_DEBUG NaN scan, Lattice.hpp:412-422); clears the flag. */
+   (the reference's LLALBM_DEBUG NaN scan, Lattice.hpp:412-422), LLB_E_TIMEOUT
+   if a pipelined kernel gave up a bounded wait; clears the flags. */
 int llb_check_numerics(llb_handle h);
 /* CUDA events on the handle's stream: slot in [0, 8). */
 int llb_event_record(llb_handle h, int32_t slot);
 int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, float* ms);
-/* Columns of lattice nodes per thread block of the step kernel (1..8; each
-   block is 32 rows x block_y columns).  A tuning knob for the autotuner. */
+/* Step-kernel selection, for the autotuner.  Plain steps run the TMA-pipelined
+   kernel in configuration `config` (0..2: tile shape, stage count, warps), or
+   the one-thread-per-node kernel for config -1.  Both compute identical
+   arithmetic. */
+int llb_set_pipeline(llb_handle h, int32_t config);
+int llb_get_pipeline(llb_handle h, int32_t* config);
+/* Columns of lattice nodes per thread block of the one-thread-per-node kernel
+   (1..8; each block is 32 rows x block_y columns). */
 int llb_set_launch_shape(llb_handle h, int32_t block_y);
 /* Device bytes held by the handle. */
 int llb_device_bytes(llb_handle h, int64_t* bytes);

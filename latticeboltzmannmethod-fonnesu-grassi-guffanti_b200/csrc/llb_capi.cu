@@ -4,6 +4,8 @@
 // resident populations (two buffers, ping-pong), the open-boundary value ring,
 // output buffers and a device step counter.  Multi-step calls are replayed from
 // CUDA graphs of GRAPH_STEPS kernels (one graph per buffer parity).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +62,14 @@ struct llb_lattice {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t bytes = 0;
     std::string err;
+    // TMA-pipelined step kernel (plain steps); tma_cfg < 0 selects the
+    // one-thread-per-node kernel.
+    int tma_cfg = 0;
+    TmaPlan plan;
+    bool maps_ready = false;
+    CUtensorMap pmap[2];  // populations f[0], f[1]
+    CUtensorMap mmap;     // node mask
+    int sm_count = 148;
 };
 
 namespace {
@@ -227,6 +237,48 @@ int ensure_partials(llb_handle h, int nblocks) {
     return LLB_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// Tensor maps of the two population buffers, (ld, C, 9) elements with boxes
+// of BI x BJ x 1, and of the mask, (ld, C) bytes with boxes of BIM x BJM.
+int build_maps(llb_handle h) {
+    if (h->maps_ready) return LLB_OK;
+    if (!tma_plan(h->storage, h->tma_cfg, &h->plan)) return fail(h, LLB_E_INVALID, "unknown pipeline configuration");
+    auto enc = tensor_map_encoder();
+    if (!enc) return fail(h, LLB_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const CUtensorMapDataType dt = h->storage == LLB_STORE_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                   : h->storage == LLB_STORE_F32S ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(h->ld), static_cast<cuuint64_t>(h->C), 9};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(h->ld) * h->elem, static_cast<cuuint64_t>(h->plane) * h->elem};
+    const cuuint32_t box[3] = {static_cast<cuuint32_t>(h->plan.BI), static_cast<cuuint32_t>(h->plan.BJ), 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int b = 0; b < 2; ++b) {
+        CUresult r = enc(&h->pmap[b], dt, 3, h->f[b], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(h, LLB_E_CUDA, "cuTensorMapEncodeTiled (populations) failed");
+    }
+    const cuuint64_t mdims[2] = {static_cast<cuuint64_t>(h->ld), static_cast<cuuint64_t>(h->C)};
+    const cuuint64_t mstrides[1] = {static_cast<cuuint64_t>(h->ld)};
+    const cuuint32_t mbox[2] = {static_cast<cuuint32_t>(h->plan.BIM), static_cast<cuuint32_t>(h->plan.BJM)};
+    CUresult r = enc(&h->mmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, h->d_mask, mdims, mstrides, mbox, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(h, LLB_E_CUDA, "cuTensorMapEncodeTiled (mask) failed");
+    h->maps_ready = true;
+    return LLB_OK;
+}
+
 // One step kernel.  Inside a graph capture the step index is relative
 // (graph_offset >= 0, base read from d_step); otherwise it is absolute.
 int launch_one(llb_handle h, bool macro, long long graph_offset = -1) {
@@ -234,6 +286,18 @@ int launch_one(llb_handle h, bool macro, long long graph_offset = -1) {
     if (graph_offset >= 0) {
         x.ss.tbase = h->d_step;
         x.ss.t_off = graph_offset;
+    }
+    if (!macro && h->tma_cfg >= 0) {
+        int rc = build_maps(h);
+        if (rc) return rc;
+        const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
+        const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
+        cudaError_t e = launch_step_tma(h->storage, h->plan, x, &h->pmap[h->cur], &h->mmap, h->f[h->cur],
+                                        h->f[h->cur ^ 1], grid);
+        if (e != cudaSuccess) return cuda_fail(h, e, "pipelined step kernel launch");
+        h->cur ^= 1;
+        ++h->step;
+        return LLB_OK;
     }
     cudaError_t e = launch_step(h->storage, x, h->f[h->cur], h->f[h->cur ^ 1], false, macro);
     if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
@@ -271,6 +335,9 @@ namespace llb {
 cudaError_t launch_step(int s, const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
     return s == LLB_STORE_F64 ? launch_step_f64(x, fin, fout, init, macro) : launch_step_lowp(s, x, fin, fout, init, macro);
 }
+cudaError_t launch_fill_keep(int s, const LaunchCtx& x, void* buf) {
+    return s == LLB_STORE_F64 ? launch_fill_keep_f64(x, buf) : launch_fill_keep_lowp(s, x, buf);
+}
 cudaError_t launch_finalize(int s, const LaunchCtx& x, const void* fin, double* out, long long t) {
     return s == LLB_STORE_F64 ? launch_finalize_f64(x, fin, out, t) : launch_finalize_lowp(s, x, fin, out, t);
 }
@@ -284,6 +351,14 @@ cudaError_t launch_flow_forces(int s, const LaunchCtx& x, const void* fin, const
                                long long n, double2* p, int nb, double* out2) {
     return s == LLB_STORE_F64 ? launch_flow_forces_f64(x, fin, pts, dirs, n, p, nb, out2)
                               : launch_flow_forces_lowp(s, x, fin, pts, dirs, n, p, nb, out2);
+}
+bool tma_plan(int s, int cfg, TmaPlan* out) {
+    return s == LLB_STORE_F64 ? tma_plan_f64(cfg, out) : tma_plan_lowp(s, cfg, out);
+}
+cudaError_t launch_step_tma(int s, const TmaPlan& p, const LaunchCtx& x, const CUtensorMap* pm, const CUtensorMap* mm,
+                            const void* fin, void* fout, int grid) {
+    return s == LLB_STORE_F64 ? launch_step_tma_f64(p, x, pm, mm, fin, fout, grid)
+                              : launch_step_tma_lowp(s, p, x, pm, mm, fin, fout, grid);
 }
 cudaError_t launch_gather_forces(int s, const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
                                  long long n, double* out) {
@@ -334,6 +409,8 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     h->plane = static_cast<long long>(h->ld) * d->cols;
     h->n_open = static_cast<int>(n_open);
     h->cap = cap;
+    // default pipeline configuration per storage form (measured on B200, porous 4096^2)
+    h->tma_cfg = d->storage == LLB_STORE_F64 ? 1 : 0;
     if (d->collision == LLB_BGK) {
         h->coll.model = 0;
         h->coll.t = 1.0 / d->tau;  // BGKCollision.hpp:142-143
@@ -359,6 +436,8 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     if ((rc = select_device(h))) return bail(rc);
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaStreamCreate"));
+    e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+    if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaDeviceGetAttribute"));
     const size_t pop_bytes = static_cast<size_t>(h->plane) * 9 * h->elem;
     const size_t N = static_cast<size_t>(h->R * h->C);
     if ((rc = dev_alloc(h, &h->f[0], pop_bytes)) || (rc = dev_alloc(h, &h->f[1], pop_bytes)) ||
@@ -373,8 +452,9 @@ int llb_create(const llb_desc* d, llb_handle* out) {
         e = cudaMemcpyAsync(h->d_open_idx, open_idx.data(), open_idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(h->d_open, 0, sizeof(double2) * static_cast<size_t>(std::max<int64_t>(n_open, 1)) * cap, h->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(h->f[0], 0, pop_bytes, h->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(h->f[1], 0, pop_bytes, h->stream);
+    // every slot starts at its direction's initial value: dead nodes keep it
+    if (e == cudaSuccess) e = launch_fill_keep(h->storage, make_ctx(h), h->f[0]);
+    if (e == cudaSuccess) e = launch_fill_keep(h->storage, make_ctx(h), h->f[1]);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "lattice upload"));
@@ -574,6 +654,7 @@ int llb_check_numerics(llb_handle h) {
     LLB_CUDA(h, cudaMemcpyAsync(&flags, h->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
     LLB_CUDA(h, cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream));
     LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (flags & 2u) return fail(h, LLB_E_TIMEOUT, "a pipelined step kernel gave up waiting for its copies");
     if (flags & 1u) return fail(h, LLB_E_NUMERIC, "non-finite density detected");
     return LLB_OK;
 }
@@ -594,6 +675,26 @@ int llb_event_elapsed_ms(llb_handle h, int32_t a, int32_t b, float* ms) {
     if (rc) return rc;
     LLB_CUDA(h, cudaEventSynchronize(h->ev[b]));
     LLB_CUDA(h, cudaEventElapsedTime(ms, h->ev[a], h->ev[b]));
+    return LLB_OK;
+}
+
+int llb_set_pipeline(llb_handle h, int32_t config) {
+    if (!h || config < -1 || config >= TMA_CONFIGS) return fail(h, LLB_E_INVALID, "config must be -1 or in [0, 3)");
+    if (config != h->tma_cfg) {
+        int rc = select_device(h);
+        if (rc) return rc;
+        LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (auto& g : h->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        h->tma_cfg = config;
+        h->maps_ready = false;
+    }
+    return LLB_OK;
+}
+
+int llb_get_pipeline(llb_handle h, int32_t* config) {
+    if (!h || !config) return fail(h, LLB_E_INVALID, "bad arguments");
+    *config = h->tma_cfg;
     return LLB_OK;
 }
 

@@ -8,6 +8,7 @@ namespace llb {
 cudaError_t launch_step_f64(const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
     return do_step<ModelF64>(x, fin, fout, init, macro);
 }
+cudaError_t launch_fill_keep_f64(const LaunchCtx& x, void* buf) { return do_fill_keep<ModelF64>(x, buf); }
 cudaError_t launch_finalize_f64(const LaunchCtx& x, const void* fin, double* out, long long t) {
     return do_finalize<ModelF64>(x, fin, out, t);
 }
@@ -22,6 +23,30 @@ cudaError_t launch_flow_forces_f64(const LaunchCtx& x, const void* fin, const in
 cudaError_t launch_gather_forces_f64(const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
                                      long long n, double* out) {
     return do_gather<ModelF64>(x, fin, pts, dirs, n, out);
+}
+
+// TMA pipeline configurations of the FP64 step (tile rows, tile columns, stages, consumer warps)
+using F64Cfg0 = TmaCfg<double, 128, 4, 4, 16>;
+using F64Cfg1 = TmaCfg<double, 128, 8, 2, 16>;
+using F64Cfg2 = TmaCfg<double, 128, 4, 4, 20>;
+
+bool tma_plan_f64(int cfg, TmaPlan* p) {
+    switch (cfg) {
+    case 0: fill_plan<ModelF64, F64Cfg0>(0, p); return true;
+    case 1: fill_plan<ModelF64, F64Cfg1>(1, p); return true;
+    case 2: fill_plan<ModelF64, F64Cfg2>(2, p); return true;
+    default: return false;
+    }
+}
+
+cudaError_t launch_step_tma_f64(const TmaPlan& p, const LaunchCtx& x, const CUtensorMap* pm, const CUtensorMap* mm,
+                                const void* fin, void* fout, int grid) {
+    switch (p.cfg) {
+    case 0: return do_step_tma<ModelF64, F64Cfg0>(x, pm, mm, fin, fout, grid);
+    case 1: return do_step_tma<ModelF64, F64Cfg1>(x, pm, mm, fin, fout, grid);
+    case 2: return do_step_tma<ModelF64, F64Cfg2>(x, pm, mm, fin, fout, grid);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace llb

@@ -18,14 +18,15 @@
 namespace llb {
 
 // ---- node mask byte ----------------------------------------------------------
-// bits 0-1  class: DEAD (never updated; as a streaming source its slot keeps the
-//           initial value), FLUID, BB (wall or wet obstacle: as a source it
-//           bounces the population back), OPEN (inlet or outlet)
-// bit  2    PLAIN: all 8 streaming sources are FLUID or OPEN (no per-direction
-//           source inspection needed)
+// bits 0-1  class: DEAD (never updated), FLUID, BB (wall or wet obstacle: as a
+//           streaming source it bounces the population back), OPEN (inlet/outlet)
+// bit  2    PLAIN: all 8 streaming sources of an active node are FLUID or OPEN
 // bits 3-5  side of an OPEN node: 0 none/corner, 1 top, 2 right, 3 bottom, 4 left
 //           (the reference's btypes TOP_WALL..LEFT_WALL)
 // bits 6-7  closure of an OPEN node: 0 Zou-He velocity, 1 none, 2 Zou-He pressure
+// Population slots of DEAD nodes always hold the initial value of their
+// direction (filled at creation, rewritten only with that value), so a pull
+// from a dead source reads the reference's never-written slot as is.
 constexpr uint8_t CLS_DEAD = 0, CLS_FLUID = 1, CLS_BB = 2, CLS_OPEN = 3;
 constexpr uint8_t MASK_PLAIN = 4;
 constexpr int SIDE_SHIFT = 3, BC_SHIFT = 6;
@@ -54,7 +55,8 @@ __host__ __device__ constexpr int opp(int k) {
 // Initial populations of every active node: the reference's equilibrium at
 // rho = 1, u = 0 (Lattice.hpp:326-328 with DefaultEquilibrium.hpp:64-76),
 // evaluated with the same expressions.  A population slot nobody streams into
-// keeps this value for the whole run.
+// keeps this value for the whole run (DEAD sources, and sources outside the
+// lattice of open nodes on its edge).
 __host__ __device__ constexpr double w_init(int k) {
     return k == 0 ? (2.0 / 9.0) * 1.0 * (2 - 3 * 0.0)
          : k <= 4 ? (1.0 / 18.0) * 1.0 * (2 + 6 * 0.0 + 9 * 0.0 * 0.0 - 3 * 0.0)

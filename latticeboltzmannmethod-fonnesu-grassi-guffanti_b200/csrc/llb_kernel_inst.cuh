@@ -3,6 +3,7 @@
 
 #include "llb_kernels.cuh"
 #include "llb_launch.h"
+#include "llb_tma.cuh"
 
 namespace llb {
 
@@ -22,6 +23,12 @@ cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, 
         else { if (macro) LLB_STEP(1, true, false); else LLB_STEP(1, false, false); }
     }
 #undef LLB_STEP
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_fill_keep(const LaunchCtx& x, void* buf) {
+    k_fill_keep<M><<<1024, 256, 0, x.stream>>>(static_cast<typename M::T*>(buf), x.g.plane);
     return cudaGetLastError();
 }
 
@@ -59,6 +66,36 @@ cudaError_t do_gather(const LaunchCtx& x, const void* fin, const int64_t* pts, c
     if (n <= 0) return cudaSuccess;
     const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
     k_gather_forces<M><<<blocks, 256, 0, x.stream>>>(x.g, static_cast<const typename M::T*>(fin), pts, dirs, n, out);
+    return cudaGetLastError();
+}
+
+// ---- TMA-pipelined step -------------------------------------------------------
+template <class M, class CFG>
+void fill_plan(int cfg, TmaPlan* p) {
+    p->cfg = cfg;
+    p->TI = CFG::TI;
+    p->TJ = CFG::TJ;
+    p->S = CFG::S;
+    p->W = CFG::W;
+    p->BI = CFG::BI;
+    p->BJ = CFG::BJ;
+    p->BIM = CFG::BIM;
+    p->BJM = CFG::BJM;
+    p->smem = CFG::SMEM_BYTES;
+    p->threads = CFG::THREADS;
+}
+
+template <class M, class CFG>
+cudaError_t do_step_tma(const LaunchCtx& x, const CUtensorMap* pmap, const CUtensorMap* mmap, const void* fin,
+                        void* fout, int grid) {
+    using T = typename M::T;
+    auto k0 = k_step_tma<M, 0, CFG>;
+    auto k1 = k_step_tma<M, 1, CFG>;
+    auto kern = x.c.model == 0 ? k0 : k1;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CFG::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, x.g, x.ot, x.c, static_cast<const T*>(fin),
+                                                             static_cast<T*>(fout), x.ss);
     return cudaGetLastError();
 }
 

@@ -8,7 +8,8 @@
 //   1. pull  S_t(x,k):  f*_{t-1}(x - c_k, k)   if the source node is fluid or open
 //                       f*_{t-1}(x, opp(k))    if it is a wall or wet obstacle
 //                                              (half-way bounce-back)
-//                       initial value w_k      if outside the lattice or dead
+//                       initial value w_k      if it is dead (its slot holds w_k)
+//                                              or outside the lattice
 //      -- the reference's push stream + bounce-back (Lattice.hpp:393-403) seen
 //         from the receiving node: every population slot has exactly one writer;
 //   2. the inlet/outlet closure with the boundary values of step t-1
@@ -30,8 +31,7 @@ __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __r
     f[0] = M::load(fin + node);
     if (m & MASK_PLAIN) {
 #pragma unroll
-        for (int k = 1; k < 9; ++k)
-            f[k] = M::load(fin + k * g.plane + node - (DJ(k) * g.ld + DI(k)));
+        for (int k = 1; k < 9; ++k) f[k] = M::load(fin + k * g.plane + node - (DJ(k) * g.ld + DI(k)));
     } else {
 #pragma unroll
         for (int k = 1; k < 9; ++k) {
@@ -39,9 +39,10 @@ __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __r
             typename M::R v = M::keep(k);
             if (si >= 0 && sj >= 0 && si < g.rows && sj < g.cols) {
                 const long long src = static_cast<long long>(sj) * g.ld + si;
-                const uint8_t sc = mask_class(g.mask[src]);
-                if (class_active(sc)) v = M::load(fin + k * g.plane + src);
-                else if (sc == CLS_BB) v = M::load(fin + opp(k) * g.plane + node);
+                // a bounce-back source reflects this node's own population; fluid,
+                // open and dead sources are read where they are
+                v = mask_class(g.mask[src]) == CLS_BB ? M::load(fin + opp(k) * g.plane + node)
+                                                      : M::load(fin + k * g.plane + src);
             }
             f[k] = v;
         }
@@ -87,8 +88,9 @@ __device__ __forceinline__ void flag_numerics(const StepSync& ss, bool bad) {
 
 // Stores of a warp cover whole 32-byte sectors when every lane of a sector
 // writes: lanes of inactive nodes that share a sector with an active node
-// store too (their value is never read), so L2 never has to merge a partial
-// sector with DRAM contents.  Lanes whose whole sector is inactive skip.
+// store the initial values too (dead slots must keep them; wall and obstacle
+// slots are never read), so L2 need not merge a partial sector with DRAM
+// contents.  Lanes whose whole sector is inactive skip.
 template <class M>
 __device__ __forceinline__ bool sector_has_active(bool active) {
     constexpr int lanes_per_sector = 32 / sizeof(typename M::T);
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
         } else {
             if (write_sector) {
 #pragma unroll
-                for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, typename M::R(0));
+                for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
             }
             if (MACRO) {
                 const long long d = static_cast<long long>(j) * g.rows + i;
@@ -160,11 +162,21 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
             }
         }
     } else if (write_sector && j < g.cols && i < g.ld) {
-        // padding rows of a column that shares a sector with active nodes
+        // padding rows (dead) of a column that shares a sector with active nodes
 #pragma unroll
-        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, typename M::R(0));
+        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
     }
     flag_numerics(ss, bad);
+}
+
+// Every slot of a population buffer set to the node-independent initial value
+// of its direction (dead nodes keep it for ever; other slots are overwritten).
+template <class M>
+__global__ void k_fill_keep(typename M::T* __restrict__ f, long long plane) {
+    const long long n = 9 * plane;
+    for (long long x = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; x < n;
+         x += static_cast<long long>(gridDim.x) * blockDim.x)
+        M::store(f + x, M::keep(static_cast<int>(x / plane)));
 }
 
 // populations S_t = stream + bounce-back + closures of the resident state,

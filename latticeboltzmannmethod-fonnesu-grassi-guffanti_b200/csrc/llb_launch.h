@@ -2,6 +2,7 @@
 // per-storage kernel translation units (llb_f64.cu, llb_lowp.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "llb_internal.cuh"
@@ -30,7 +31,11 @@ cudaError_t launch_flow_forces(int storage, const LaunchCtx& ctx, const void* fi
 cudaError_t launch_gather_forces(int storage, const LaunchCtx& ctx, const void* fin, const int64_t* pts,
                                  const uint16_t* dirs, long long n, double* out);
 
+cudaError_t launch_fill_keep(int storage, const LaunchCtx& ctx, void* buf);
+
 // per translation unit
+cudaError_t launch_fill_keep_f64(const LaunchCtx&, void*);
+cudaError_t launch_fill_keep_lowp(int storage, const LaunchCtx&, void*);
 cudaError_t launch_step_f64(const LaunchCtx&, const void*, void*, bool, bool);
 cudaError_t launch_finalize_f64(const LaunchCtx&, const void*, double*, long long);
 cudaError_t launch_export_f64(const LaunchCtx&, const void*, double*);
@@ -47,6 +52,29 @@ cudaError_t launch_flow_forces_lowp(int storage, const LaunchCtx&, const void*, 
                                     long long, double2*, int, double*);
 cudaError_t launch_gather_forces_lowp(int storage, const LaunchCtx&, const void*, const int64_t*,
                                       const uint16_t*, long long, double*);
+
+// One configuration of the TMA-pipelined step kernel (tile TI x TJ nodes,
+// S shared-memory stages, W consumer warps + 1 producer warp).
+struct TmaPlan {
+    int cfg = -1;
+    int TI = 0, TJ = 0, S = 0, W = 0;
+    int BI = 0;            // rows of a population box
+    int BJ = 0;            // columns of a population box
+    int BIM = 0, BJM = 0;  // rows / columns of the mask box
+    int smem = 0;          // dynamic shared memory bytes
+    int threads = 0;
+};
+constexpr int TMA_CONFIGS = 3;
+// Fills `out` for configuration `cfg` (0..TMA_CONFIGS-1) of a storage form.
+bool tma_plan(int storage, int cfg, TmaPlan* out);
+cudaError_t launch_step_tma(int storage, const TmaPlan& p, const LaunchCtx& ctx, const CUtensorMap* pmap,
+                            const CUtensorMap* mmap, const void* fin, void* fout, int grid);
+bool tma_plan_f64(int cfg, TmaPlan* out);
+cudaError_t launch_step_tma_f64(const TmaPlan&, const LaunchCtx&, const CUtensorMap*, const CUtensorMap*,
+                                const void*, void*, int);
+bool tma_plan_lowp(int storage, int cfg, TmaPlan* out);
+cudaError_t launch_step_tma_lowp(int storage, const TmaPlan&, const LaunchCtx&, const CUtensorMap*,
+                                 const CUtensorMap*, const void*, void*, int);
 
 inline dim3 node_grid(const Geometry& g, int bx, int by) {
     return dim3(static_cast<unsigned>((g.rows + bx - 1) / bx), static_cast<unsigned>((g.cols + by - 1) / by));

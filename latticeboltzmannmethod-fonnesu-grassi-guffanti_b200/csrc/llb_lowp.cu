@@ -15,6 +15,9 @@ using ModelF16S = ModelShift<__half>;
 cudaError_t launch_step_lowp(int storage, const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
     LLB_DISPATCH((do_step<ModelF32S>(x, fin, fout, init, macro)), (do_step<ModelF16S>(x, fin, fout, init, macro)));
 }
+cudaError_t launch_fill_keep_lowp(int storage, const LaunchCtx& x, void* buf) {
+    LLB_DISPATCH((do_fill_keep<ModelF32S>(x, buf)), (do_fill_keep<ModelF16S>(x, buf)));
+}
 cudaError_t launch_finalize_lowp(int storage, const LaunchCtx& x, const void* fin, double* out, long long t) {
     LLB_DISPATCH((do_finalize<ModelF32S>(x, fin, out, t)), (do_finalize<ModelF16S>(x, fin, out, t)));
 }
@@ -33,6 +36,49 @@ cudaError_t launch_flow_forces_lowp(int storage, const LaunchCtx& x, const void*
 cudaError_t launch_gather_forces_lowp(int storage, const LaunchCtx& x, const void* fin, const int64_t* pts,
                                       const uint16_t* dirs, long long n, double* out) {
     LLB_DISPATCH((do_gather<ModelF32S>(x, fin, pts, dirs, n, out)), (do_gather<ModelF16S>(x, fin, pts, dirs, n, out)));
+}
+
+// TMA pipeline configurations (tile rows, tile columns, stages, consumer warps)
+using F32Cfg0 = TmaCfg<float, 128, 8, 4, 16>;
+using F32Cfg1 = TmaCfg<float, 128, 4, 6, 16>;
+using F32Cfg2 = TmaCfg<float, 128, 8, 4, 20>;
+using F16Cfg0 = TmaCfg<__half, 128, 16, 3, 16>;
+using F16Cfg1 = TmaCfg<__half, 128, 8, 6, 16>;
+using F16Cfg2 = TmaCfg<__half, 128, 16, 4, 20>;
+
+bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
+    if (storage == LLB_STORE_F32S) {
+        switch (cfg) {
+        case 0: fill_plan<ModelF32S, F32Cfg0>(0, p); return true;
+        case 1: fill_plan<ModelF32S, F32Cfg1>(1, p); return true;
+        case 2: fill_plan<ModelF32S, F32Cfg2>(2, p); return true;
+        default: return false;
+        }
+    }
+    switch (cfg) {
+    case 0: fill_plan<ModelF16S, F16Cfg0>(0, p); return true;
+    case 1: fill_plan<ModelF16S, F16Cfg1>(1, p); return true;
+    case 2: fill_plan<ModelF16S, F16Cfg2>(2, p); return true;
+    default: return false;
+    }
+}
+
+cudaError_t launch_step_tma_lowp(int storage, const TmaPlan& p, const LaunchCtx& x, const CUtensorMap* pm,
+                                 const CUtensorMap* mm, const void* fin, void* fout, int grid) {
+    if (storage == LLB_STORE_F32S) {
+        switch (p.cfg) {
+        case 0: return do_step_tma<ModelF32S, F32Cfg0>(x, pm, mm, fin, fout, grid);
+        case 1: return do_step_tma<ModelF32S, F32Cfg1>(x, pm, mm, fin, fout, grid);
+        case 2: return do_step_tma<ModelF32S, F32Cfg2>(x, pm, mm, fin, fout, grid);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (p.cfg) {
+    case 0: return do_step_tma<ModelF16S, F16Cfg0>(x, pm, mm, fin, fout, grid);
+    case 1: return do_step_tma<ModelF16S, F16Cfg1>(x, pm, mm, fin, fout, grid);
+    case 2: return do_step_tma<ModelF16S, F16Cfg2>(x, pm, mm, fin, fout, grid);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace llb

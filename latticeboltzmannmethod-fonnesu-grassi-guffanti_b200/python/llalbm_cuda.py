@@ -92,6 +92,8 @@ SIGNATURES = {
     "llb_check_numerics": [_H],
     "llb_event_record": [_H, ctypes.c_int32],
     "llb_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
+    "llb_set_pipeline": [_H, ctypes.c_int32],
+    "llb_get_pipeline": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_set_launch_shape": [_H, ctypes.c_int32],
     "llb_device_bytes": [_H, ctypes.POINTER(ctypes.c_int64)],
 }
@@ -270,6 +272,16 @@ class CudaLattice:
         ms = ctypes.c_float()
         _check(lib().llb_event_elapsed_ms(self._h, a, b, ctypes.byref(ms)), self._h)
         return float(ms.value)
+
+    def set_pipeline(self, config: int):
+        """0..2: TMA-pipelined step configurations; -1: one thread per node."""
+        _check(lib().llb_set_pipeline(self._h, config), self._h)
+
+    @property
+    def pipeline(self) -> int:
+        c = ctypes.c_int32()
+        _check(lib().llb_get_pipeline(self._h, ctypes.byref(c)), self._h)
+        return c.value
 
     def set_launch_shape(self, block_y: int):
         _check(lib().llb_set_launch_shape(self._h, block_y), self._h)

@@ -12,14 +12,17 @@ import harness as H
 pytestmark = pytest.mark.gpu
 
 
-def make_gpu(lists: H.NodeLists, p: H.Params, storage=0, table_rows=1):
+def make_gpu(lists: H.NodeLists, p: H.Params, storage=0, table_rows=1, pipeline=None):
     import llalbm_cuda as L
 
-    return L.CudaLattice(lists.rows, lists.cols, lists.fluid, lists.wall, lists.inlet, lists.inlet_side,
+    g = L.CudaLattice(lists.rows, lists.cols, lists.fluid, lists.wall, lists.inlet, lists.inlet_side,
                          lists.outlet, lists.outlet_side, lists.obstacle, lists.obstacle_dirs,
                          collision=p.collision, tau=p.tau, tau_even=p.tau_even, tau_odd=p.tau_odd,
                          inlet_bc=p.inlet_bc, outlet_bc=p.outlet_bc, storage=storage,
                          open_table_rows=table_rows)
+    if pipeline is not None:
+        g.set_pipeline(pipeline)
+    return g
 
 
 def pressure_table(table: np.ndarray, lists: H.NodeLists, p: H.Params) -> np.ndarray:
@@ -32,10 +35,10 @@ def pressure_table(table: np.ndarray, lists: H.NodeLists, p: H.Params) -> np.nda
     return t
 
 
-def run_gpu(lists, p, steps, table, storage=0):
+def run_gpu(lists, p, steps, table, storage=0, pipeline=None):
     tab = pressure_table(table, lists, p)
     rows = tab.shape[0]
-    with make_gpu(lists, p, storage=storage, table_rows=max(rows, 1)) as g:
+    with make_gpu(lists, p, storage=storage, table_rows=max(rows, 1), pipeline=pipeline) as g:
         if lists.n_open:
             g.set_open_values(tab, 0)
         g.init(macro=(steps == 1))
@@ -87,6 +90,35 @@ def test_f64_bit_exact(case, steps):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
+@pytest.mark.parametrize("pipeline", [-1, 0, 1, 2])
+@pytest.mark.parametrize("case", [CASES[2], CASES[5], CASES[6]], ids=[CASES[2][0], CASES[5][0], CASES[6][0]])
+def test_f64_every_step_kernel_bit_exact(case, pipeline):
+    """The one-thread-per-node kernel (-1) and every TMA pipeline configuration."""
+    name, lists, p, ins, outs = case
+    steps = 150
+    table = H.open_values(lists, ins, outs, steps)
+    ref = H.run_oracle(lists, p, steps, table)
+    got = run_gpu(lists, p, steps, table, pipeline=pipeline)
+    act = H.active_mask(lists)
+    np.testing.assert_array_equal(got["populations"][:, act], ref["populations"][:, act])
+    np.testing.assert_array_equal(got["u"], ref["u"])
+
+
+def test_f64_pipeline_large_lattice_bit_exact():
+    """A lattice with many tiles per CTA (porous 512 x 640, several tile rows and
+    columns, ragged last tiles) through the pipelined kernel vs the simple one."""
+    lists = H.classify(H.porous_types(500, 640, seed=3))
+    p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.02:0", "pressure", 1)
+    outs = []
+    for pipeline in (-1, 0, 1, 2):
+        outs.append(run_gpu(lists, p, 60, table, pipeline=pipeline))
+    act = H.active_mask(lists)
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o["populations"][:, act], outs[0]["populations"][:, act])
+        np.testing.assert_array_equal(o["post"][:, act], outs[0]["post"][:, act])
+
+
 def test_cavity129_10k_steps_bit_exact():
     """Config 1 (129x129 lid cavity, BGK tau 0.884, lid u = (0.1, 0)) after 10 000 steps."""
     lists = H.classify(H.cavity_types(129))
@@ -105,14 +137,15 @@ def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
+@pytest.mark.parametrize("pipeline", [-1, 0, 1, 2])
 @pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3)], ids=["f32s", "f16s"])
-def test_shifted_storage_velocity_error(storage, tol):
+def test_shifted_storage_velocity_error(storage, tol, pipeline):
     lists = H.classify(H.channel_types(64, 160, discs=[(32, 40, 8)]))
     p = H.Params.trt_magic(0.56, outlet_bc=H.BC_ZH_PRESSURE)
     table = H.open_values(lists, "parabolic:0.05:1:62", "pressure", 1)
     steps = 2000
     ref = H.run_oracle(lists, p, steps, table)
-    got = run_gpu(lists, p, steps, table, storage=storage)
+    got = run_gpu(lists, p, steps, table, storage=storage, pipeline=pipeline)
     err = rel_l2(got["u"], ref["u"])
     assert err <= tol, err
 
