@@ -172,6 +172,23 @@ int llb_flow_forces(llb_handle h, double lift_drag[2]);
    values[n][8] (0 where the bit is clear), for feeding the reference analyzer. */
 int llb_gather_force_inputs(llb_handle h, double* values);
 
+/* Allocation-free variant of llb_set_force_points + llb_flow_forces; it has no
+   counterpart in the reference.  For callers that cannot let the library call
+   cudaMalloc once their loop runs -- a server whose device memory is committed
+   up front under a fixed budget, or a host that must not trigger the
+   device-wide synchronisation cudaMalloc/cudaFree can cause: the points and
+   the per-block partial sums go to one static device array of
+   LLB_NOALLOC_MAX_FORCE_POINTS points (about 1.2 MB per device, reserved when
+   the library loads) instead of buffers allocated per call.  Same per-point
+   terms and summation order as llb_flow_forces.  More than the maximum points
+   fails with LLB_E_INVALID.  The first call on a device looks the array up
+   (cudaGetSymbolAddress) and should come before any stream capture on that
+   device.  All calls share the array: calls that overlap on the GPU race and
+   must be serialised by the caller. */
+#define LLB_NOALLOC_MAX_FORCE_POINTS 65536
+int llb_flow_forces_noalloc(llb_handle h, const int64_t* ij, const uint16_t* dirs, int64_t n,
+                            double lift_drag[2]);
+
 /* Mass and momentum of the resident post-collision state (sum over fluid,
    inlet and outlet nodes of sum_k f, c_x f, c_y f) with compensated FP64;
    out[0] = mass, out[1] = momentum along j (u_x), out[2] = along -i (u_y). */

@@ -28,6 +28,7 @@ SOURCES = {
     "llb_f64.cu": ["--fmad=false"],
     "llb_lowp.cu": [],
     "llb_capi.cu": [],
+    "llb_noalloc.cu": [],
     "llb_classify.cpp": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [

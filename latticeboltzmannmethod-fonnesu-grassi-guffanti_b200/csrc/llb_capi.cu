@@ -367,6 +367,26 @@ cudaError_t launch_gather_forces(int s, const LaunchCtx& x, const void* fin, con
 }
 }  // namespace llb
 
+// Hooks for llb_noalloc.cu: the launch context of a handle's resident state
+// (with its device made current) and its error reporting.
+namespace llb {
+int handle_force_context(llb_handle h, LaunchCtx* ctx, const void** fin, double** d_out, int* storage,
+                         int* device, int64_t* rows, int64_t* cols) {
+    if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
+    int rc = select_device(h);
+    if (rc) return rc;
+    *ctx = make_ctx(h);
+    *fin = h->f[h->cur];
+    *d_out = h->d_red;
+    *storage = h->storage;
+    *device = h->device;
+    *rows = h->R;
+    *cols = h->C;
+    return LLB_OK;
+}
+int handle_fail(llb_handle h, int code, const char* msg) { return fail(h, code, msg); }
+}  // namespace llb
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------

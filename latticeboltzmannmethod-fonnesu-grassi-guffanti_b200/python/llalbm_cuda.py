@@ -87,6 +87,7 @@ SIGNATURES = {
     "llb_set_force_points": [_H, _P, _P, ctypes.c_int64],
     "llb_flow_forces": [_H, _P],
     "llb_gather_force_inputs": [_H, _P],
+    "llb_flow_forces_noalloc": [_H, _P, _P, ctypes.c_int64, _P],
     "llb_mass_momentum": [_H, _P],
     "llb_synchronize": [_H],
     "llb_check_numerics": [_H],
@@ -252,6 +253,13 @@ class CudaLattice:
     def flow_forces(self):
         out = np.zeros(2)
         _check(lib().llb_flow_forces(self._h, _ptr(out)), self._h)
+        return float(out[0]), float(out[1])
+
+    def flow_forces_noalloc(self, pts, dirs):
+        """Lift and drag without device allocation (static scratch, <= 65536 points)."""
+        p = _ij(pts); q = np.ascontiguousarray(np.asarray(dirs, dtype=np.uint16).reshape(-1))
+        out = np.zeros(2)
+        _check(lib().llb_flow_forces_noalloc(self._h, _ptr(p), _ptr(q), len(p), _ptr(out)), self._h)
         return float(out[0]), float(out[1])
 
     def gather_force_inputs(self) -> np.ndarray:
