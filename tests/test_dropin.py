@@ -1,0 +1,87 @@
+"""The C++ drop-in: LLALBM programs built with CUDAPolicy instead of SerialPolicy.
+
+The example programs (package examples/) use LLALBM's own Lattice API; each is
+built twice from the same source, differing only in the parallelization-policy
+template argument.  The CUDA build must reproduce the reference's serial build
+bit for bit: populations of fluid/inlet/outlet nodes, u, rho, the saved u files
+and the FlowAnalyzer lift/drag series.  The serial build is itself checked
+against the C oracle.
+"""
+import filecmp
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import harness as H
+
+BIN = os.path.join(H.ROOT, "latticeboltzmannmethod-fonnesu-grassi-guffanti_b200", "examples", "_bin")
+needs_bins = pytest.mark.skipif(not os.path.exists(os.path.join(BIN, "lid_driven_cavity_serial")),
+                                reason="example programs not built (the reference headers were absent)")
+
+
+def run(exe, args, cwd):
+    os.makedirs(cwd, exist_ok=True)
+    p = subprocess.run([os.path.join(BIN, exe), *args], cwd=cwd, capture_output=True, text=True, timeout=900)
+    assert p.returncode == 0, p.stdout[-1000:] + p.stderr[-1000:]
+    return {n: np.fromfile(os.path.join(cwd, n + ".f64")) for n in ("populations", "u", "rho", "lift_drag")
+            if os.path.exists(os.path.join(cwd, n + ".f64"))}
+
+
+def active_flat(lists):
+    a = H.active_mask(lists)  # (C, R)
+    return np.tile(a.reshape(-1), 9)
+
+
+@needs_bins
+def test_serial_example_matches_oracle(tmp_path):
+    lists = H.classify(H.cavity_types(129))
+    lat = str(tmp_path / "lid.txt")
+    H.write_lattice_file(lat, H.cavity_types(129))
+    out = run("lid_driven_cavity_serial", [lat, "200", "0", str(tmp_path / "s")], str(tmp_path / "s"))
+    ref = H.run_oracle(lists, H.Params(tau=0.884), 200, H.open_values(lists, "const:0.1:0", "const:0:0", 1))
+    act = active_flat(lists)
+    np.testing.assert_array_equal(out["populations"][act], ref["populations"].reshape(-1)[act])
+    np.testing.assert_array_equal(out["u"], ref["u"].reshape(-1))
+
+
+@needs_bins
+@pytest.mark.gpu
+@pytest.mark.parametrize("steps,save,ramp", [(1000, 0, False), (600, 150, True)], ids=["const", "ramp_saves"])
+def test_cuda_policy_matches_serial_policy_lid(tmp_path, steps, save, ramp):
+    lat = str(tmp_path / "lid.txt")
+    H.write_lattice_file(lat, H.cavity_types(129))
+    lists = H.classify(H.cavity_types(129))
+    extra = ["ramp"] if ramp else []
+    outs = {}
+    for pol in ("serial", "cuda"):
+        d = str(tmp_path / pol)
+        outs[pol] = run(f"lid_driven_cavity_{pol}", [lat, str(steps), str(save), d, *extra], d)
+    act = active_flat(lists)
+    np.testing.assert_array_equal(outs["cuda"]["populations"][act], outs["serial"]["populations"][act])
+    np.testing.assert_array_equal(outs["cuda"]["u"], outs["serial"]["u"])
+    np.testing.assert_array_equal(outs["cuda"]["rho"], outs["serial"]["rho"])
+    if save:
+        files = sorted(os.listdir(tmp_path / "serial" / "results"))
+        assert len(files) == 2 * (steps // save)
+        for f in files:
+            assert filecmp.cmp(tmp_path / "serial" / "results" / f, tmp_path / "cuda" / "results" / f, shallow=False), f
+
+
+@needs_bins
+@pytest.mark.gpu
+def test_cuda_policy_matches_serial_policy_cylinder_with_analyzer(tmp_path):
+    types = H.cylinder_types(64, 160, x0=40, y0=33, r=8)
+    lat = str(tmp_path / "cyl.txt")
+    H.write_lattice_file(lat, types)
+    lists = H.classify(types)
+    outs = {}
+    for pol in ("serial", "cuda"):
+        d = str(tmp_path / pol)
+        outs[pol] = run(f"cylinder_flow_{pol}", [lat, "400", "0.56", "0.05", d], d)
+    act = active_flat(lists)
+    np.testing.assert_array_equal(outs["cuda"]["populations"][act], outs["serial"]["populations"][act])
+    np.testing.assert_array_equal(outs["cuda"]["u"], outs["serial"]["u"])
+    assert len(outs["serial"]["lift_drag"]) == 2 * 39
+    np.testing.assert_array_equal(outs["cuda"]["lift_drag"], outs["serial"]["lift_drag"])
