@@ -358,13 +358,98 @@ def run_ours(a, dist):
     return line, wl, types
 
 
+def batch_add(b, L, prob, storage):
+    """Adds one config-4 problem to a batch (or creates it alone when b is None)."""
+    types = prob["make_types"]()
+    n = L.classify(types)
+    ni, no = len(n["inlet"]), len(n["outlet"])
+    tab = np.zeros((1, ni + no, 2))
+    tab[0, :ni, 0] = prob["u"]
+    if prob["outlet_bc"] == 2:
+        tab[0, ni:] = (1.0, 0.0)
+    kw = dict(collision=1 if prob["trt"] else 0, tau=prob["tau"], tau_even=prob["tau"], tau_odd=prob["tau_odd"],
+              outlet_bc=prob["outlet_bc"])
+    R, C = types.shape
+    args = (R, C, n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"], n["outlet_side"],
+            n["obstacle"], n["obstacle_dirs"])
+    active = len(n["fluid"]) + ni + no
+    if b is None:
+        g = L.CudaLattice(*args, storage=storage, **kw)
+        g.set_open_values(tab)
+        return g, active
+    return b.add(*args, open_values=tab, **kw), active
+
+
+def run_batch(a, dist):
+    """Config 4: 256 uneven problems advanced as one batch (FP32-shifted,
+    autotuned launch shape) against each problem alone through the plain FP64
+    path."""
+    import llalbm_cuda as L
+
+    probs = W.batch_problems()
+    nodes = sum(p["rows"] * p["cols"] for p in probs)
+    b = L.CudaBatch(storage=L.STORE_F32S, device=dist.local)
+    active = 0
+    for p in probs:
+        _, act = batch_add(b, L, p, L.STORE_F32S)
+        active += act
+    by, spl, tune_ms = b.tune(8)
+    b.step(a.warmup)
+    b.synchronize()
+    dist.barrier()
+    sampler = ClockSampler(dist.local)
+    t0 = time.perf_counter()
+    b.record(0)
+    b.step(a.steps)
+    b.record(1)
+    b.synchronize()
+    t1 = time.perf_counter()
+    ms = dist.max(b.elapsed_ms(0, 1))
+    sampler.stop()
+    batched = dist.world * nodes * a.steps / ms / 1e3
+    b.close()
+    # plain FP64 path, one problem at a time, same lattices
+    k_plain = max(1, min(a.steps, 40))
+    plain_ms = 0.0
+    for p in probs:
+        g, _ = batch_add(None, L, p, L.STORE_F64)
+        g.init()
+        g.step(3)
+        g.synchronize()
+        g.record(0)
+        g.step(k_plain)
+        g.record(1)
+        plain_ms += g.elapsed_ms(0, 1)
+        g.close()
+    plain = nodes * k_plain / plain_ms / 1e3
+    bps = 18 * 4 * active + nodes
+    peak = (json.load(open(PEAKS_FILE)).get("hbm_gbs") if os.path.exists(PEAKS_FILE) else None) or FALLBACK_HBM_GBS
+    per = ms / a.steps
+    return {
+        "metric": METRIC, "value": round(batched, 1), "unit": "MLUPS", "n_gpus": dist.world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(per, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (shifted storage)", "data": "synthetic",
+        "config": {"workload": "batch256", "lattices": len(probs), "nodes": nodes, "active_nodes": active,
+                   "description": "256 problems, nx 64..1024 step 32, aspect 1..4, half lid cavities, half "
+                                  "channels with 0-8 discs, tau U[0.55,1.5], BGK/TRT 50/50",
+                   "launch": {"block_y": by, "steps_per_launch": spl, "autotuned_ms_per_step": round(tune_ms, 4)}},
+        "roofline": {"bound": "hbm", "achieved": round(bps / per / 1e6, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(bps / per / 1e6 / peak, 4), "traffic": None},
+        "plain_f64": {"mlups": round(plain, 1), "steps_per_problem": k_plain,
+                      "path": "each problem alone through llb_step (FP64, TMA pipeline)"},
+        "batched_over_plain_f64": round(batched / plain, 3),
+        "gpu_launches": (a.steps + spl - 1) // spl, "clocks": sampler.summary(t0, t1),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", default="porous4096", choices=("porous4096", "cylinder1024x256", "cavity129"))
+    ap.add_argument("--workload", default="porous4096",
+                    choices=("porous4096", "cylinder1024x256", "cavity129", "batch256"))
     ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous workload")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -395,6 +480,12 @@ def main():
         return
 
     dist = Dist(a.gpus)
+    if a.workload == "batch256":
+        line = run_batch(a, dist)
+        if dist.rank == 0:
+            print(json.dumps(line), flush=True)
+        dist.close()
+        return
     line, wl, types = run_ours(a, dist)
     if dist.rank == 0:
         if dist.world == 1 and not a.no_cpu_baseline:

@@ -154,6 +154,10 @@ int llb_get_step(llb_handle h, int64_t* step);
 /* global_rho / global_u of the last LLB_STEP_MACRO step (Lattice.hpp:58-70 getters
    :499-506); either pointer may be NULL. */
 int llb_get_macro(llb_handle h, double* rho, double* u);
+/* rho and u of the current populations S_t (t = llb_get_step): what the next
+   step's macro output would write, without stepping (fluid moments; the
+   prescribed or Zou-He values of open nodes; rho 1 and u 0 elsewhere). */
+int llb_compute_macro(llb_handle h, double* rho, double* u);
 /* `populations` (Lattice.hpp:492): streams the resident post-collision state
    and applies bounce-back and the closures into an (R, C, 9) tensor.  Values
    are defined for fluid, inlet and outlet nodes; other nodes read 0. */
@@ -193,6 +197,43 @@ int llb_flow_forces_noalloc(llb_handle h, const int64_t* ij, const uint16_t* dir
    inlet and outlet nodes of sum_k f, c_x f, c_y f) with compensated FP64;
    out[0] = mass, out[1] = momentum along j (u_x), out[2] = along -i (u_y). */
 int llb_mass_momentum(llb_handle h, double out[3]);
+
+/* ---- batches of lattices ------------------------------------------------ */
+/* Many independent lattices (uneven sizes, BGK or TRT, own relaxation times,
+   one storage form) advanced together by one persistent launch per step over
+   a work list of lattice tiles -- or per several steps, launched
+   cooperatively -- replayed from CUDA graphs.  There is no counterpart in the
+   reference (its statics allow one parameter set per process); a batch is
+   what a solve server runs.  Lattices join (llb_batch_add: creation, boundary
+   values for steps 0.., step 0) and leave between calls.  Each lattice is an
+   llb_handle sharing the batch's stream: read its results with the
+   single-lattice calls on llb_batch_lattice's handle.  Stepping a lattice
+   through that handle is allowed; the batch picks up its new step. */
+typedef struct llb_batch* llb_batch_handle;
+int llb_batch_create(int32_t device, int32_t storage, llb_batch_handle* out);
+int llb_batch_destroy(llb_batch_handle b);
+int llb_batch_add(llb_batch_handle b, const llb_desc* desc, const double* open_values, int32_t rows,
+                  int32_t* slot);
+int llb_batch_remove(llb_batch_handle b, int32_t slot);
+/* Advances every lattice of the batch by nsteps. */
+int llb_batch_step(llb_batch_handle b, int32_t nsteps);
+int llb_batch_lattice(llb_batch_handle b, int32_t slot, llb_handle* out);
+/* Launch shape: tile columns per block (1..8) and steps per launch (1: one
+   launch per step, replayed from graphs; >1: cooperative multi-step launches). */
+int llb_batch_set_config(llb_batch_handle b, int32_t block_y, int32_t steps_per_launch);
+int llb_batch_get_config(llb_batch_handle b, int32_t* block_y, int32_t* steps_per_launch);
+/* Autotuner: times trial_steps real steps of the batch for every candidate
+   shape (the steps advance the lattices; every candidate computes the same
+   arithmetic) and keeps the fastest. */
+int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, int32_t* steps_per_launch,
+                   float* ms_per_step);
+int llb_batch_get_step(llb_batch_handle b, int64_t* step);
+/* Waits for the batch; LLB_E_TIMEOUT if a cooperative launch gave up a grid barrier. */
+int llb_batch_synchronize(llb_batch_handle b);
+int llb_batch_event_record(llb_batch_handle b, int32_t slot);
+int llb_batch_event_elapsed_ms(llb_batch_handle b, int32_t slot_begin, int32_t slot_end, float* ms);
+int llb_batch_info(llb_batch_handle b, int64_t* lattices, int64_t* nodes, int64_t* device_bytes);
+const char* llb_batch_last_error(llb_batch_handle b);
 
 /* ---- synchronisation, timing, errors ------------------------------------ */
 

@@ -1,0 +1,442 @@
+// Batches of lattices (C ABI llb_batch_*): independent D2Q9 problems of uneven
+// sizes, collision models and relaxation times advanced together, one
+// persistent launch per step (or per several steps, cooperatively), replayed
+// from CUDA graphs.  Lattices can join and leave between calls: a solve server
+// admits requests into a running batch as memory frees up.
+//
+// Every lattice of a batch is an ordinary llb_handle (created by llb_create,
+// stepped to step 0 by llb_init) whose stream is the batch's stream, so its
+// results are read with the single-lattice calls (llb_get_populations,
+// llb_compute_macro, llb_flow_forces, ...).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/llalbm_cuda.h"
+#include "llb_batch.cuh"
+#include "llb_handle.h"
+#include "llb_launch.h"
+
+using namespace llb;
+
+namespace {
+constexpr int BATCH_GRAPH_STEPS = 32;
+}
+
+struct llb_batch {
+    int device = 0;
+    int storage = LLB_STORE_F32S;
+    cudaStream_t stream = nullptr;
+    int sm_count = 148;
+    std::vector<llb_handle> slot;        // nullptr: free slot
+    std::vector<BatchLattice> desc;      // per slot
+    std::vector<int> order;              // active slots in descriptor order
+    BatchLattice* d_desc = nullptr;
+    int desc_cap = 0;
+    int2* d_items = nullptr;
+    int items_cap = 0;
+    int n_items = 0;
+    long long step = 0;                  // batch step counter
+    long long* d_sbase = nullptr;
+    unsigned* d_bar = nullptr;           // [count, generation]
+    unsigned* d_err = nullptr;
+    int block_y = 4;
+    int spl = 1;                         // steps per launch
+    bool dirty = true;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev[8] = {};
+    std::string err;
+};
+
+namespace {
+
+int bfail(llb_batch_handle b, int code, const std::string& m) {
+    if (b) b->err = m;
+    return code;
+}
+
+#define LLB_BCUDA(b, call)                                                               \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return bfail(b, e_ == cudaErrorMemoryAllocation ? LLB_E_NOMEM : LLB_E_CUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));            \
+    } while (0)
+
+void drop_graph(llb_batch_handle b) {
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+}
+
+// Per-lattice step and buffer implied by the batch counter.
+void sync_handle(llb_batch_handle b, int s) {
+    llb_handle h = b->slot[s];
+    const BatchLattice& d = b->desc[s];
+    const long long delta = b->step - d.s0;
+    h->step = d.t0 + delta;
+    h->cur = d.cur0 ^ static_cast<int>(delta & 1);
+}
+
+// A lattice stepped through its own handle since the last batch call is
+// re-anchored at its current step and buffer.
+void reanchor_if_moved(llb_batch_handle b, int s) {
+    llb_handle h = b->slot[s];
+    BatchLattice& d = b->desc[s];
+    const long long delta = b->step - d.s0;
+    if (h->step != d.t0 + delta || h->cur != (d.cur0 ^ static_cast<int>(delta & 1))) {
+        d.t0 = h->step;
+        d.s0 = b->step;
+        d.cur0 = h->cur;
+        b->dirty = true;
+    }
+}
+
+int rebuild(llb_batch_handle b) {
+    if (!b->dirty) return LLB_OK;
+    drop_graph(b);
+    b->order.clear();
+    std::vector<BatchLattice> dev;
+    std::vector<int2> items;
+    for (int s = 0; s < static_cast<int>(b->slot.size()); ++s) {
+        if (!b->slot[s]) continue;
+        const int idx = static_cast<int>(dev.size());
+        b->order.push_back(s);
+        dev.push_back(b->desc[s]);
+        const BatchLattice& d = b->desc[s];
+        const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
+        for (int t = 0; t < d.nti * ntj; ++t) items.push_back(make_int2(idx, t));
+    }
+    LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+    if (static_cast<int>(dev.size()) > b->desc_cap) {
+        if (b->d_desc) cudaFree(b->d_desc);
+        b->desc_cap = std::max<int>(static_cast<int>(dev.size()), 2 * b->desc_cap);
+        LLB_BCUDA(b, cudaMalloc(&b->d_desc, sizeof(BatchLattice) * b->desc_cap));
+    }
+    if (static_cast<int>(items.size()) > b->items_cap) {
+        if (b->d_items) cudaFree(b->d_items);
+        b->items_cap = std::max<int>(static_cast<int>(items.size()), 2 * b->items_cap);
+        LLB_BCUDA(b, cudaMalloc(&b->d_items, sizeof(int2) * b->items_cap));
+    }
+    if (!dev.empty())
+        LLB_BCUDA(b, cudaMemcpyAsync(b->d_desc, dev.data(), sizeof(BatchLattice) * dev.size(), cudaMemcpyHostToDevice,
+                                     b->stream));
+    if (!items.empty())
+        LLB_BCUDA(b, cudaMemcpyAsync(b->d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice,
+                                     b->stream));
+    LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->n_items = static_cast<int>(items.size());
+    b->dirty = false;
+    return LLB_OK;
+}
+
+BatchLaunch launch_desc(llb_batch_handle b, long long soff, int steps) {
+    BatchLaunch L{};
+    L.lats = b->d_desc;
+    L.items = b->d_items;
+    L.n_items = b->n_items;
+    L.sbase = b->d_sbase;
+    L.soff = soff;
+    L.steps = steps;
+    L.bar = b->d_bar;
+    L.err = b->d_err;
+    L.block_y = b->block_y;
+    L.stream = b->stream;
+    L.cooperative = steps > 1;
+    const int maxg = batch_max_grid(b->storage, b->block_y, b->sm_count);
+    L.grid = std::max(1, std::min(b->n_items, maxg > 0 ? maxg : b->sm_count));
+    return L;
+}
+
+int set_base(llb_batch_handle b) {
+    LLB_BCUDA(b, cudaMemcpyAsync(b->d_sbase, &b->step, sizeof(long long), cudaMemcpyHostToDevice, b->stream));
+    return LLB_OK;
+}
+
+int launch_steps(llb_batch_handle b, int32_t nsteps) {
+    int rc;
+    if (b->n_items == 0) {
+        b->step += nsteps;
+        return LLB_OK;
+    }
+    if (b->spl > 1) {
+        // cooperative launches of spl steps each, then the remainder one by one
+        while (nsteps > 0) {
+            const int k = std::min<int>(nsteps, b->spl);
+            if ((rc = set_base(b))) return rc;
+            cudaError_t e = launch_batch_step(b->storage, launch_desc(b, 0, k));
+            if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
+            b->step += k;
+            nsteps -= k;
+        }
+        return LLB_OK;
+    }
+    if (nsteps >= BATCH_GRAPH_STEPS) {
+        if (!b->graph) {
+            cudaGraph_t g = nullptr;
+            LLB_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t le = cudaSuccess;
+            for (int s = 0; s < BATCH_GRAPH_STEPS && le == cudaSuccess; ++s)
+                le = launch_batch_step(b->storage, launch_desc(b, s, 1));
+            cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+            if (le != cudaSuccess || ee != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return bfail(b, LLB_E_CUDA, "capture of the batched step graph failed");
+            }
+            cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return bfail(b, LLB_E_CUDA, "cudaGraphInstantiate (batch)");
+        }
+        while (nsteps >= BATCH_GRAPH_STEPS) {
+            if ((rc = set_base(b))) return rc;
+            LLB_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
+            b->step += BATCH_GRAPH_STEPS;
+            nsteps -= BATCH_GRAPH_STEPS;
+        }
+    }
+    if (nsteps > 0) {
+        if ((rc = set_base(b))) return rc;
+        for (int s = 0; s < nsteps; ++s) {
+            cudaError_t e = launch_batch_step(b->storage, launch_desc(b, s, 1));
+            if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
+        }
+        b->step += nsteps;
+    }
+    return LLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int llb_batch_create(int32_t device, int32_t storage, llb_batch_handle* out) {
+    if (!out || storage < LLB_STORE_F64 || storage > LLB_STORE_F16S) return LLB_E_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return LLB_E_NODEVICE;
+    llb_batch_handle b = new (std::nothrow) llb_batch();
+    if (!b) return LLB_E_NOMEM;
+    b->device = device;
+    b->storage = storage;
+    auto bail = [&](int rc) {
+        llb_batch_destroy(b);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(LLB_E_CUDA);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(LLB_E_CUDA);
+    cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMalloc(&b->d_sbase, sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&b->d_bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->d_err, sizeof(unsigned)) != cudaSuccess)
+        return bail(LLB_E_NOMEM);
+    if (cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), b->stream) != cudaSuccess ||
+        cudaMemsetAsync(b->d_err, 0, sizeof(unsigned), b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return bail(LLB_E_CUDA);
+    *out = b;
+    return LLB_OK;
+}
+
+int llb_batch_destroy(llb_batch_handle b) {
+    if (!b) return LLB_E_INVALID;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (llb_handle h : b->slot)
+        if (h) llb_destroy(h);
+    drop_graph(b);
+    for (void* p : {static_cast<void*>(b->d_desc), static_cast<void*>(b->d_items), static_cast<void*>(b->d_sbase),
+                    static_cast<void*>(b->d_bar), static_cast<void*>(b->d_err)})
+        if (p) cudaFree(p);
+    for (auto& e : b->ev)
+        if (e) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return LLB_OK;
+}
+
+int llb_batch_add(llb_batch_handle b, const llb_desc* desc, const double* open_values, int32_t rows, int32_t* slot) {
+    if (!b || !desc || !slot) return LLB_E_INVALID;
+    if (desc->storage != b->storage || desc->pattern != LLB_PATTERN_AB || desc->device != b->device)
+        return bfail(b, LLB_E_INVALID, "lattice storage, pattern or device differs from the batch");
+    if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    llb_handle h = nullptr;
+    int rc = llb_create(desc, &h);
+    if (rc != LLB_OK) return bfail(b, rc, llb_last_error(nullptr));
+    // the lattice works on the batch's stream from now on
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+    h->stream = b->stream;
+    h->own_stream = false;
+    h->tma_cfg = -1;
+    if (open_values && rows > 0 && (rc = llb_set_open_values(h, 0, rows, open_values)) != LLB_OK) {
+        llb_destroy(h);
+        return bfail(b, rc, "boundary values rejected");
+    }
+    if ((rc = llb_init(h, 0)) != LLB_OK) {
+        llb_destroy(h);
+        return bfail(b, rc, "llb_init failed");
+    }
+    BatchLattice d{};
+    const LaunchCtx x = handle_ctx(h);
+    d.g = x.g;
+    d.ot = x.ot;
+    d.c = x.c;
+    d.f[0] = h->f[0];
+    d.f[1] = h->f[1];
+    d.t0 = h->step;
+    d.s0 = b->step;
+    d.cur0 = h->cur;
+    d.nti = static_cast<int>((h->R + BX - 1) / BX);
+    d.flags = h->d_flags;
+    int s = 0;
+    while (s < static_cast<int>(b->slot.size()) && b->slot[s]) ++s;
+    if (s == static_cast<int>(b->slot.size())) {
+        b->slot.push_back(nullptr);
+        b->desc.push_back(BatchLattice{});
+    }
+    b->slot[s] = h;
+    b->desc[s] = d;
+    b->dirty = true;
+    *slot = s;
+    return LLB_OK;
+}
+
+int llb_batch_remove(llb_batch_handle b, int32_t slot) {
+    if (!b || slot < 0 || slot >= static_cast<int>(b->slot.size()) || !b->slot[slot]) return LLB_E_INVALID;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    llb_destroy(b->slot[slot]);
+    b->slot[slot] = nullptr;
+    b->dirty = true;
+    return LLB_OK;
+}
+
+int llb_batch_step(llb_batch_handle b, int32_t nsteps) {
+    if (!b || nsteps < 0) return LLB_E_INVALID;
+    if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    for (int s = 0; s < static_cast<int>(b->slot.size()); ++s)
+        if (b->slot[s]) reanchor_if_moved(b, s);
+    int rc = rebuild(b);
+    if (rc != LLB_OK) return rc;
+    if ((rc = launch_steps(b, nsteps)) != LLB_OK) return rc;
+    for (int s = 0; s < static_cast<int>(b->slot.size()); ++s)
+        if (b->slot[s]) sync_handle(b, s);
+    return LLB_OK;
+}
+
+int llb_batch_lattice(llb_batch_handle b, int32_t slot, llb_handle* out) {
+    if (!b || !out || slot < 0 || slot >= static_cast<int>(b->slot.size()) || !b->slot[slot]) return LLB_E_INVALID;
+    sync_handle(b, slot);
+    *out = b->slot[slot];
+    return LLB_OK;
+}
+
+int llb_batch_set_config(llb_batch_handle b, int32_t block_y, int32_t steps_per_launch) {
+    if (!b || block_y < 1 || block_y > MAX_BLOCK_Y || steps_per_launch < 1 || steps_per_launch > 1024)
+        return LLB_E_INVALID;
+    if (block_y != b->block_y) b->dirty = true;
+    b->block_y = block_y;
+    b->spl = steps_per_launch;
+    drop_graph(b);
+    return LLB_OK;
+}
+
+int llb_batch_get_config(llb_batch_handle b, int32_t* block_y, int32_t* steps_per_launch) {
+    if (!b || !block_y || !steps_per_launch) return LLB_E_INVALID;
+    *block_y = b->block_y;
+    *steps_per_launch = b->spl;
+    return LLB_OK;
+}
+
+int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, int32_t* steps_per_launch,
+                   float* ms_per_step) {
+    if (!b || trial_steps < 1) return LLB_E_INVALID;
+    if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    static const int shapes[] = {1, 2, 4, 8};
+    static const int spls[] = {1, 8};
+    float best = 1e30f;
+    int best_by = b->block_y, best_spl = b->spl;
+    for (int e = 0; e < 2; ++e)
+        if (!b->ev[e]) LLB_BCUDA(b, cudaEventCreate(&b->ev[e]));
+    for (int by : shapes) {
+        for (int spl : spls) {
+            int rc = llb_batch_set_config(b, by, spl);
+            if (rc != LLB_OK) return rc;
+            if ((rc = llb_batch_step(b, std::min(trial_steps, 8))) != LLB_OK) return rc;  // graph capture, warm-up
+            LLB_BCUDA(b, cudaEventRecord(b->ev[0], b->stream));
+            if ((rc = llb_batch_step(b, trial_steps)) != LLB_OK) return rc;
+            LLB_BCUDA(b, cudaEventRecord(b->ev[1], b->stream));
+            LLB_BCUDA(b, cudaEventSynchronize(b->ev[1]));
+            float ms = 0.f;
+            LLB_BCUDA(b, cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+            if (ms < best) {
+                best = ms;
+                best_by = by;
+                best_spl = spl;
+            }
+        }
+    }
+    int rc = llb_batch_set_config(b, best_by, best_spl);
+    if (rc != LLB_OK) return rc;
+    if (block_y) *block_y = best_by;
+    if (steps_per_launch) *steps_per_launch = best_spl;
+    if (ms_per_step) *ms_per_step = best / static_cast<float>(trial_steps);
+    return LLB_OK;
+}
+
+int llb_batch_get_step(llb_batch_handle b, int64_t* step) {
+    if (!b || !step) return LLB_E_INVALID;
+    *step = b->step;
+    return LLB_OK;
+}
+
+int llb_batch_synchronize(llb_batch_handle b) {
+    if (!b) return LLB_E_INVALID;
+    cudaSetDevice(b->device);
+    LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+    unsigned err = 0;
+    LLB_BCUDA(b, cudaMemcpy(&err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (err) {
+        cudaMemset(b->d_err, 0, sizeof(unsigned));
+        return bfail(b, LLB_E_TIMEOUT, "batched kernel gave up a grid barrier");
+    }
+    return LLB_OK;
+}
+
+int llb_batch_event_record(llb_batch_handle b, int32_t slot) {
+    if (!b || slot < 0 || slot >= 8) return LLB_E_INVALID;
+    cudaSetDevice(b->device);
+    if (!b->ev[slot]) LLB_BCUDA(b, cudaEventCreate(&b->ev[slot]));
+    LLB_BCUDA(b, cudaEventRecord(b->ev[slot], b->stream));
+    return LLB_OK;
+}
+
+int llb_batch_event_elapsed_ms(llb_batch_handle b, int32_t a, int32_t c, float* ms) {
+    if (!b || !ms || a < 0 || a >= 8 || c < 0 || c >= 8 || !b->ev[a] || !b->ev[c]) return LLB_E_INVALID;
+    LLB_BCUDA(b, cudaEventSynchronize(b->ev[c]));
+    LLB_BCUDA(b, cudaEventElapsedTime(ms, b->ev[a], b->ev[c]));
+    return LLB_OK;
+}
+
+int llb_batch_info(llb_batch_handle b, int64_t* lattices, int64_t* nodes, int64_t* device_bytes) {
+    if (!b) return LLB_E_INVALID;
+    int64_t n = 0, nn = 0, bytes = 0;
+    for (llb_handle h : b->slot) {
+        if (!h) continue;
+        ++n;
+        nn += h->R * h->C;
+        bytes += h->bytes;
+    }
+    if (lattices) *lattices = n;
+    if (nodes) *nodes = nn;
+    if (device_bytes) *device_bytes = bytes;
+    return LLB_OK;
+}
+
+const char* llb_batch_last_error(llb_batch_handle b) { return b ? b->err.c_str() : ""; }
+
+}  // extern "C"

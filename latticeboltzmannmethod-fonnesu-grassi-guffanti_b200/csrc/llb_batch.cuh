@@ -1,0 +1,162 @@
+// Batched step: many independent lattices (uneven sizes, BGK or TRT, own tau)
+// advanced by one persistent launch.
+//
+// Every lattice is described by a BatchLattice in device memory; the work list
+// holds one item per (lattice, tile of 32 rows x blockDim.y columns).  A
+// persistent grid walks the items with a grid-stride loop, so lattices of any
+// size share the launch and the load balances at tile granularity.  A lattice
+// joins the batch at batch step s0 with its step index t0 and current buffer
+// cur0; at batch step s it is at step t0 + (s - s0) and reads buffer
+// cur0 ^ ((s - s0) & 1), so lattices that joined at different times coexist and
+// no per-step bookkeeping is written.
+//
+// With steps > 1 one launch advances all lattices several steps, separated by a
+// grid barrier; the host launches it cooperatively (all blocks co-resident).
+// The barrier's spin is bounded: on timeout it raises the batch error flag and
+// the kernel returns.
+#pragma once
+
+#include "llb_kernels.cuh"
+
+namespace llb {
+
+struct BatchLattice {
+    Geometry g;
+    OpenTable ot;
+    Collision c;
+    void* f[2];
+    long long t0;   // lattice step index at batch step s0
+    long long s0;
+    int cur0;       // buffer holding the lattice's state at batch step s0
+    int nti;        // row tiles: ceil(rows / 32)
+    unsigned* flags;
+};
+
+constexpr long long BARRIER_LIMIT = 1LL << 22;
+constexpr unsigned BATCH_FLAG_TIMEOUT = 1u;
+
+// Generation barrier across the grid (blocks must be co-resident).
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks) {
+    __shared__ int ok_sh;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        volatile unsigned* vgen = gen;
+        const unsigned g0 = *vgen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(count, 1u) == nblocks - 1) {
+            *count = 0u;
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            long long it = 0;
+            while (*vgen == g0) {
+                if (++it > BARRIER_LIMIT) { ok = 0; break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_sh = ok;
+    }
+    __syncthreads();
+    return ok_sh != 0;
+}
+
+template <class M>
+__device__ __forceinline__ void batch_tile(const BatchLattice& L, int tile, long long s) {
+    using T = typename M::T;
+    const long long d = s - L.s0;
+    const int cur = L.cur0 ^ static_cast<int>(d & 1);
+    const long long t = L.t0 + d;
+    const T* __restrict__ fin = static_cast<const T*>(L.f[cur]);
+    T* __restrict__ fout = static_cast<T*>(L.f[cur ^ 1]);
+    const Geometry& g = L.g;
+    const int i = (tile % L.nti) * BX + threadIdx.x;
+    const int j = (tile / L.nti) * blockDim.y + threadIdx.y;
+    const bool inside = i < g.rows && j < g.cols;
+    const long long node = static_cast<long long>(j) * g.ld + i;
+    const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
+    const uint8_t cls = mask_class(m);
+    const bool write_sector = sector_has_active<M>(class_active(cls));
+    bool bad = false;
+    if (inside && class_active(cls)) {
+        typename M::R f[9];
+        pull<M>(g, fin, i, j, node, m, f);
+        double rho, ux, uy;
+        typename M::R rr;
+        if (cls == CLS_OPEN) {
+            open_node<M>(L.ot, g.open_idx[node], m, t, f, rho, ux, uy);
+            rr = M::from_f64(rho);
+        } else {
+            typename M::R r, x, y;
+            M::moments(f, r, x, y);
+            rr = r;
+            ux = x;
+            uy = y;
+            bad = !isfinite(M::rho_f64(r));
+        }
+        if (L.c.model == 0) M::template collide<0>(f, rr, ux, uy, L.c);
+        else M::template collide<1>(f, rr, ux, uy, L.c);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
+    } else if (write_sector && j < g.cols && i < g.ld) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(L.flags, 1u);
+}
+
+// One launch: `steps` batch steps starting at batch step (*sbase + soff).
+template <class M>
+__global__ void __launch_bounds__(BX* BY) k_batch_step(const BatchLattice* __restrict__ lats,
+                                                       const int2* __restrict__ items, int n_items,
+                                                       const long long* sbase, long long soff, int steps,
+                                                       unsigned* bar, unsigned* err) {
+    const long long s0 = *sbase + soff;
+    for (int st = 0; st < steps; ++st) {
+        const long long s = s0 + st;
+        for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+            const int2 it = items[item];
+            batch_tile<M>(lats[it.x], it.y, s);
+        }
+        if (st + 1 < steps && !grid_barrier(bar, bar + 1, gridDim.x)) {
+            if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(err, BATCH_FLAG_TIMEOUT);
+            return;
+        }
+    }
+}
+
+// rho and u of the current populations S_t of one lattice (pull, closure,
+// moments or prescribed values), dense (R, C) and (R, C, 2).
+template <class M>
+__global__ void __launch_bounds__(BX* BY) k_macro_now(Geometry g, OpenTable ot, const typename M::T* __restrict__ fin,
+                                                     long long t, double* __restrict__ rho_out,
+                                                     double* __restrict__ u_out) {
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= g.rows || j >= g.cols) return;
+    const long long node = static_cast<long long>(j) * g.ld + i;
+    const long long dd = static_cast<long long>(j) * g.rows + i;
+    const long long N = static_cast<long long>(g.rows) * g.cols;
+    const uint8_t m = g.mask[node];
+    const uint8_t cls = mask_class(m);
+    double rho = 1.0, ux = 0.0, uy = 0.0;
+    if (class_active(cls)) {
+        typename M::R f[9];
+        pull<M>(g, fin, i, j, node, m, f);
+        if (cls == CLS_OPEN) {
+            open_node<M>(ot, g.open_idx[node], m, t, f, rho, ux, uy);
+        } else {
+            typename M::R r, x, y;
+            M::moments(f, r, x, y);
+            rho = M::rho_f64(r);
+            ux = x;
+            uy = y;
+        }
+    }
+    rho_out[dd] = rho;
+    u_out[dd] = ux;
+    u_out[dd + N] = uy;
+}
+
+}  // namespace llb

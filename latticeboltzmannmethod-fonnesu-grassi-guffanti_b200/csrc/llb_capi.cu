@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/llalbm_cuda.h"
+#include "llb_handle.h"
 #include "llb_launch.h"
 
 using namespace llb;
@@ -27,50 +28,6 @@ thread_local std::string g_last_error;
 
 }  // namespace
 
-struct llb_lattice {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int storage = LLB_STORE_F64, pattern = LLB_PATTERN_AB;
-    int64_t R = 0, C = 0;
-    int ld = 0;
-    long long plane = 0;
-    size_t elem = 8;
-    void* f[2] = {nullptr, nullptr};
-    int cur = 0;
-    uint8_t* d_mask = nullptr;
-    int32_t* d_open_idx = nullptr;
-    double2* d_open = nullptr;
-    int n_open = 0, cap = 1;
-    double* d_rho = nullptr;
-    double* d_u = nullptr;
-    double* d_dense = nullptr;
-    long long* d_step = nullptr;  // step index at the start of a graph replay
-    unsigned* d_flags = nullptr;
-    int block_y = 4;
-    double2* d_partials = nullptr;
-    int partial_blocks = 0;
-    double* d_red = nullptr;
-    int64_t* d_fpts = nullptr;
-    uint16_t* d_fdirs = nullptr;
-    int64_t n_fpts = 0;
-    double* d_gather = nullptr;
-    Collision coll{};
-    int64_t step = 0;
-    bool initialized = false;
-    bool macro_valid = false;
-    cudaEvent_t ev[8] = {};
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int64_t bytes = 0;
-    std::string err;
-    // TMA-pipelined step kernel (plain steps); tma_cfg < 0 selects the
-    // one-thread-per-node kernel.
-    int tma_cfg = 0;
-    TmaPlan plan;
-    bool maps_ready = false;
-    CUtensorMap pmap[2];  // populations f[0], f[1]
-    CUtensorMap mmap;     // node mask
-    int sm_count = 148;
-};
 
 namespace {
 
@@ -139,7 +96,7 @@ void release(llb_handle h) {
         if (b) cudaFree(b);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
 }
 
@@ -335,6 +292,15 @@ namespace llb {
 cudaError_t launch_step(int s, const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
     return s == LLB_STORE_F64 ? launch_step_f64(x, fin, fout, init, macro) : launch_step_lowp(s, x, fin, fout, init, macro);
 }
+cudaError_t launch_batch_step(int s, const BatchLaunch& b) {
+    return s == LLB_STORE_F64 ? launch_batch_step_f64(b) : launch_batch_step_lowp(s, b);
+}
+int batch_max_grid(int s, int block_y, int sm_count) {
+    return s == LLB_STORE_F64 ? batch_max_grid_f64(block_y, sm_count) : batch_max_grid_lowp(s, block_y, sm_count);
+}
+cudaError_t launch_macro_now(int s, const LaunchCtx& x, const void* fin, long long t, double* rho, double* u) {
+    return s == LLB_STORE_F64 ? launch_macro_now_f64(x, fin, t, rho, u) : launch_macro_now_lowp(s, x, fin, t, rho, u);
+}
 cudaError_t launch_fill_keep(int s, const LaunchCtx& x, void* buf) {
     return s == LLB_STORE_F64 ? launch_fill_keep_f64(x, buf) : launch_fill_keep_lowp(s, x, buf);
 }
@@ -385,6 +351,7 @@ int handle_force_context(llb_handle h, LaunchCtx* ctx, const void** fin, double*
     return LLB_OK;
 }
 int handle_fail(llb_handle h, int code, const char* msg) { return fail(h, code, msg); }
+LaunchCtx handle_ctx(llb_handle h) { return make_ctx(h); }
 }  // namespace llb
 
 // ---------------------------------------------------------------------------
@@ -563,6 +530,21 @@ int llb_get_macro(llb_handle h, double* rho, double* u) {
     if (!h->macro_valid) return fail(h, LLB_E_STATE, "no step has written rho/u yet");
     int rc = select_device(h);
     if (rc) return rc;
+    const size_t N = static_cast<size_t>(h->R * h->C);
+    if (rho) LLB_CUDA(h, cudaMemcpyAsync(rho, h->d_rho, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
+    if (u) LLB_CUDA(h, cudaMemcpyAsync(u, h->d_u, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return LLB_OK;
+}
+
+int llb_compute_macro(llb_handle h, double* rho, double* u) {
+    if (!h || (!rho && !u)) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
+    int rc = select_device(h);
+    if (rc) return rc;
+    LaunchCtx x = make_ctx(h);
+    cudaError_t e = launch_macro_now(h->storage, x, h->f[h->cur], h->step, h->d_rho, h->d_u);
+    if (e != cudaSuccess) return cuda_fail(h, e, "macro kernel launch");
     const size_t N = static_cast<size_t>(h->R * h->C);
     if (rho) LLB_CUDA(h, cudaMemcpyAsync(rho, h->d_rho, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
     if (u) LLB_CUDA(h, cudaMemcpyAsync(u, h->d_u, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, h->stream));

@@ -49,4 +49,10 @@ cudaError_t launch_step_tma_f64(const TmaPlan& p, const LaunchCtx& x, const CUte
     }
 }
 
+cudaError_t launch_batch_step_f64(const BatchLaunch& b) { return do_batch_step<ModelF64>(b); }
+int batch_max_grid_f64(int block_y, int sm_count) { return do_batch_max_grid<ModelF64>(block_y, sm_count); }
+cudaError_t launch_macro_now_f64(const LaunchCtx& x, const void* fin, long long t, double* rho, double* u) {
+    return do_macro_now<ModelF64>(x, fin, t, rho, u);
+}
+
 }  // namespace llb

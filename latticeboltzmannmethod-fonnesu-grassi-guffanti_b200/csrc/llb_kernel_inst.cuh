@@ -4,6 +4,7 @@
 #include "llb_kernels.cuh"
 #include "llb_launch.h"
 #include "llb_tma.cuh"
+#include "llb_batch.cuh"
 
 namespace llb {
 
@@ -96,6 +97,42 @@ cudaError_t do_step_tma(const LaunchCtx& x, const CUtensorMap* pmap, const CUten
     if (e != cudaSuccess) return e;
     kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, x.g, x.ot, x.c, static_cast<const T*>(fin),
                                                              static_cast<T*>(fout), x.ss);
+    return cudaGetLastError();
+}
+
+// ---- batched step ----------------------------------------------------------------
+template <class M>
+cudaError_t do_batch_step(const BatchLaunch& b) {
+    const dim3 block(BX, b.block_y);
+    auto kern = k_batch_step<M>;
+    if (!b.cooperative) {
+        kern<<<b.grid, block, 0, b.stream>>>(b.lats, b.items, b.n_items, b.sbase, b.soff, b.steps, b.bar, b.err);
+        return cudaGetLastError();
+    }
+    const BatchLattice* lats = b.lats;
+    const int2* items = b.items;
+    int n_items = b.n_items;
+    const long long* sbase = b.sbase;
+    long long soff = b.soff;
+    int steps = b.steps;
+    unsigned* bar = b.bar;
+    unsigned* err = b.err;
+    void* args[] = {&lats, &items, &n_items, &sbase, &soff, &steps, &bar, &err};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kern), dim3(b.grid), block, args, 0, b.stream);
+}
+
+template <class M>
+int do_batch_max_grid(int block_y, int sm_count) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<M>, BX * block_y, 0) != cudaSuccess)
+        return 0;
+    return per_sm * sm_count;
+}
+
+template <class M>
+cudaError_t do_macro_now(const LaunchCtx& x, const void* fin, long long t, double* rho, double* u) {
+    k_macro_now<M><<<node_grid(x.g, BX, BY), dim3(BX, BY), 0, x.stream>>>(
+        x.g, x.ot, static_cast<const typename M::T*>(fin), t, rho, u);
     return cudaGetLastError();
 }
 

@@ -33,7 +33,35 @@ cudaError_t launch_gather_forces(int storage, const LaunchCtx& ctx, const void* 
 
 cudaError_t launch_fill_keep(int storage, const LaunchCtx& ctx, void* buf);
 
+struct BatchLattice;
+// Batched step over a work list (llb_batch.cuh).  `cooperative` launches the
+// grid cooperatively (required when steps > 1).
+struct BatchLaunch {
+    const BatchLattice* lats;
+    const int2* items;
+    int n_items;
+    const long long* sbase;
+    long long soff;
+    int steps;
+    unsigned* bar;
+    unsigned* err;
+    int grid;
+    int block_y;
+    bool cooperative;
+    cudaStream_t stream;
+};
+cudaError_t launch_batch_step(int storage, const BatchLaunch& b);
+// Largest co-resident grid of the batched kernel for a block of 32 x block_y.
+int batch_max_grid(int storage, int block_y, int sm_count);
+cudaError_t launch_macro_now(int storage, const LaunchCtx& ctx, const void* fin, long long t, double* rho, double* u);
+
 // per translation unit
+cudaError_t launch_batch_step_f64(const BatchLaunch&);
+cudaError_t launch_batch_step_lowp(int storage, const BatchLaunch&);
+int batch_max_grid_f64(int block_y, int sm_count);
+int batch_max_grid_lowp(int storage, int block_y, int sm_count);
+cudaError_t launch_macro_now_f64(const LaunchCtx&, const void*, long long, double*, double*);
+cudaError_t launch_macro_now_lowp(int storage, const LaunchCtx&, const void*, long long, double*, double*);
 cudaError_t launch_fill_keep_f64(const LaunchCtx&, void*);
 cudaError_t launch_fill_keep_lowp(int storage, const LaunchCtx&, void*);
 cudaError_t launch_step_f64(const LaunchCtx&, const void*, void*, bool, bool);

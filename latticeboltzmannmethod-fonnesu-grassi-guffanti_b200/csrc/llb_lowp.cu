@@ -81,4 +81,15 @@ cudaError_t launch_step_tma_lowp(int storage, const TmaPlan& p, const LaunchCtx&
     }
 }
 
+cudaError_t launch_batch_step_lowp(int storage, const BatchLaunch& b) {
+    LLB_DISPATCH((do_batch_step<ModelF32S>(b)), (do_batch_step<ModelF16S>(b)));
+}
+int batch_max_grid_lowp(int storage, int block_y, int sm_count) {
+    LLB_DISPATCH((do_batch_max_grid<ModelF32S>(block_y, sm_count)), (do_batch_max_grid<ModelF16S>(block_y, sm_count)));
+}
+cudaError_t launch_macro_now_lowp(int storage, const LaunchCtx& x, const void* fin, long long t, double* rho,
+                                  double* u) {
+    LLB_DISPATCH((do_macro_now<ModelF32S>(x, fin, t, rho, u)), (do_macro_now<ModelF16S>(x, fin, t, rho, u)));
+}
+
 }  // namespace llb

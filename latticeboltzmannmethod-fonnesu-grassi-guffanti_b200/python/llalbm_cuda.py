@@ -96,6 +96,24 @@ SIGNATURES = {
     "llb_set_pipeline": [_H, ctypes.c_int32],
     "llb_get_pipeline": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_set_launch_shape": [_H, ctypes.c_int32],
+    "llb_compute_macro": [_H, _P, _P],
+    "llb_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_H)],
+    "llb_batch_destroy": [_H],
+    "llb_batch_add": [_H, ctypes.POINTER(_Desc), _P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
+    "llb_batch_remove": [_H, ctypes.c_int32],
+    "llb_batch_step": [_H, ctypes.c_int32],
+    "llb_batch_lattice": [_H, ctypes.c_int32, ctypes.POINTER(_H)],
+    "llb_batch_set_config": [_H, ctypes.c_int32, ctypes.c_int32],
+    "llb_batch_get_config": [_H, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+    "llb_batch_tune": [_H, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                       ctypes.POINTER(ctypes.c_float)],
+    "llb_batch_get_step": [_H, ctypes.POINTER(ctypes.c_int64)],
+    "llb_batch_synchronize": [_H],
+    "llb_batch_event_record": [_H, ctypes.c_int32],
+    "llb_batch_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
+    "llb_batch_info": [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                       ctypes.POINTER(ctypes.c_int64)],
+    "llb_batch_last_error": [_H],
     "llb_device_bytes": [_H, ctypes.POINTER(ctypes.c_int64)],
 }
 
@@ -110,7 +128,7 @@ def lib() -> ctypes.CDLL:
         for name, args in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_char_p if name == "llb_last_error" else ctypes.c_int
+            fn.restype = ctypes.c_char_p if name.endswith("last_error") else ctypes.c_int
         _lib = L
     return _lib
 
@@ -150,8 +168,38 @@ def classify(types: np.ndarray) -> dict:
     return out
 
 
+def _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs, *,
+          collision, tau, tau_even, tau_odd, inlet_bc, outlet_bc, storage, pattern, device, open_table_rows):
+    """Descriptor plus the arrays it points into (keep them alive while it is used)."""
+    keep = {
+        "fluid": _ij(fluid), "wall": _ij(wall), "inlet": _ij(inlet), "outlet": _ij(outlet),
+        "obstacle": _ij(obstacle),
+        "inlet_side": np.ascontiguousarray(np.asarray(inlet_side, dtype=np.int32).reshape(-1)),
+        "outlet_side": np.ascontiguousarray(np.asarray(outlet_side, dtype=np.int32).reshape(-1)),
+    }
+    keep["obstacle_dirs"] = (None if obstacle_dirs is None else
+                             np.ascontiguousarray(np.asarray(obstacle_dirs, dtype=np.uint16).reshape(-1)))
+    d = _Desc(int(rows), int(cols),
+              len(keep["fluid"]), _ptr(keep["fluid"]), len(keep["wall"]), _ptr(keep["wall"]),
+              len(keep["inlet"]), _ptr(keep["inlet"]), _ptr(keep["inlet_side"]),
+              len(keep["outlet"]), _ptr(keep["outlet"]), _ptr(keep["outlet_side"]),
+              len(keep["obstacle"]), _ptr(keep["obstacle"]), _ptr(keep["obstacle_dirs"]),
+              inlet_bc, outlet_bc, collision, tau, tau_even, tau_odd, storage, pattern, device, open_table_rows)
+    return d, keep
+
+
 class CudaLattice:
     """One D2Q9 lattice resident on a GPU (the engine behind CUDAPolicy)."""
+
+    @classmethod
+    def _wrap(cls, handle, rows, cols, storage, n_inlet, n_outlet, n_active):
+        """Non-owning view of a handle that belongs to a batch."""
+        obj = cls.__new__(cls)
+        obj.rows, obj.cols, obj.storage = rows, cols, storage
+        obj.n_inlet, obj.n_outlet = n_inlet, n_outlet
+        obj.n_open, obj.n_active = n_inlet + n_outlet, n_active
+        obj._h, obj._owner, obj._force_n = handle, False, 0
+        return obj
 
     def __init__(self, rows: int, cols: int, fluid, wall, inlet, inlet_side, outlet, outlet_side,
                  obstacle, obstacle_dirs=None, *, collision: int = BGK, tau: float = 0.6,
@@ -160,24 +208,14 @@ class CudaLattice:
                  device: int = 0, open_table_rows: int = 1):
         self.rows, self.cols = int(rows), int(cols)
         self.storage = storage
-        keep = {
-            "fluid": _ij(fluid), "wall": _ij(wall), "inlet": _ij(inlet), "outlet": _ij(outlet),
-            "obstacle": _ij(obstacle),
-            "inlet_side": np.ascontiguousarray(np.asarray(inlet_side, dtype=np.int32).reshape(-1)),
-            "outlet_side": np.ascontiguousarray(np.asarray(outlet_side, dtype=np.int32).reshape(-1)),
-        }
-        keep["obstacle_dirs"] = (None if obstacle_dirs is None else
-                                 np.ascontiguousarray(np.asarray(obstacle_dirs, dtype=np.uint16).reshape(-1)))
+        self._owner = True
+        d, keep = _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs,
+                        collision=collision, tau=tau, tau_even=tau_even, tau_odd=tau_odd, inlet_bc=inlet_bc,
+                        outlet_bc=outlet_bc, storage=storage, pattern=pattern, device=device,
+                        open_table_rows=open_table_rows)
         self.n_inlet, self.n_outlet = len(keep["inlet"]), len(keep["outlet"])
         self.n_open = self.n_inlet + self.n_outlet
         self.n_active = len(keep["fluid"]) + self.n_open
-        d = _Desc(self.rows, self.cols,
-                  len(keep["fluid"]), _ptr(keep["fluid"]), len(keep["wall"]), _ptr(keep["wall"]),
-                  self.n_inlet, _ptr(keep["inlet"]), _ptr(keep["inlet_side"]),
-                  self.n_outlet, _ptr(keep["outlet"]), _ptr(keep["outlet_side"]),
-                  len(keep["obstacle"]), _ptr(keep["obstacle"]), _ptr(keep["obstacle_dirs"]),
-                  inlet_bc, outlet_bc, collision, tau, tau_even, tau_odd, storage, pattern, device,
-                  open_table_rows)
         h = ctypes.c_void_p()
         _check(lib().llb_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
@@ -186,7 +224,8 @@ class CudaLattice:
     # -- lifetime --------------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None):
-            lib().llb_destroy(self._h)
+            if getattr(self, "_owner", True):
+                lib().llb_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -233,6 +272,12 @@ class CudaLattice:
     def macro(self):
         rho = np.empty((self.cols, self.rows)); u = np.empty((2, self.cols, self.rows))
         _check(lib().llb_get_macro(self._h, _ptr(rho), _ptr(u)), self._h)
+        return rho, u
+
+    def compute_macro(self):
+        """rho, u of the current populations without stepping."""
+        rho = np.empty((self.cols, self.rows)); u = np.empty((2, self.cols, self.rows))
+        _check(lib().llb_compute_macro(self._h, _ptr(rho), _ptr(u)), self._h)
         return rho, u
 
     def populations(self) -> np.ndarray:
@@ -306,3 +351,107 @@ def from_types(types: np.ndarray, **kw) -> CudaLattice:
     R, C = types.shape
     return CudaLattice(R, C, n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"], n["outlet_side"],
                        n["obstacle"], n["obstacle_dirs"], **kw)
+
+
+def _bcheck(rc: int, b):
+    if rc != LLB_OK:
+        msg = lib().llb_batch_last_error(b) if b else b""
+        raise LLBError(rc, msg.decode() if msg else "")
+
+
+class CudaBatch:
+    """Many lattices advanced together (persistent batched launch, CUDA graphs)."""
+
+    def __init__(self, storage: int = STORE_F32S, device: int = 0):
+        b = ctypes.c_void_p()
+        _check(lib().llb_batch_create(device, storage, ctypes.byref(b)))
+        self._b, self.storage, self.device = b, storage, device
+        self._meta = {}
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().llb_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs=None, *,
+            collision=BGK, tau=0.6, tau_even=0.6, tau_odd=0.6, inlet_bc=BC_ZH_VELOCITY, outlet_bc=BC_ZH_VELOCITY,
+            open_values=None) -> int:
+        vals = None if open_values is None else np.ascontiguousarray(open_values, dtype=np.float64)
+        nrows = 0 if vals is None else vals.reshape(-1, len(inlet) + len(outlet), 2).shape[0]
+        d, keep = _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs,
+                        collision=collision, tau=tau, tau_even=tau_even, tau_odd=tau_odd, inlet_bc=inlet_bc,
+                        outlet_bc=outlet_bc, storage=self.storage, pattern=PATTERN_AB, device=self.device,
+                        open_table_rows=max(nrows, 1))
+        slot = ctypes.c_int32()
+        _bcheck(lib().llb_batch_add(self._b, ctypes.byref(d), _ptr(vals), nrows, ctypes.byref(slot)), self._b)
+        n_in, n_out = len(keep["inlet"]), len(keep["outlet"])
+        self._meta[slot.value] = (int(rows), int(cols), n_in, n_out, len(keep["fluid"]) + n_in + n_out)
+        return slot.value
+
+    def add_types(self, types, **kw) -> int:
+        n = classify(types)
+        R, C = types.shape
+        return self.add(R, C, n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"], n["outlet_side"],
+                        n["obstacle"], n["obstacle_dirs"], **kw)
+
+    def remove(self, slot: int):
+        _bcheck(lib().llb_batch_remove(self._b, slot), self._b)
+        self._meta.pop(slot, None)
+
+    def step(self, n: int = 1):
+        _bcheck(lib().llb_batch_step(self._b, n), self._b)
+
+    def lattice(self, slot: int) -> CudaLattice:
+        h = ctypes.c_void_p()
+        _bcheck(lib().llb_batch_lattice(self._b, slot, ctypes.byref(h)), self._b)
+        R, C, ni, no, na = self._meta[slot]
+        return CudaLattice._wrap(h, R, C, self.storage, ni, no, na)
+
+    def set_config(self, block_y: int, steps_per_launch: int = 1):
+        _bcheck(lib().llb_batch_set_config(self._b, block_y, steps_per_launch), self._b)
+
+    @property
+    def config(self):
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        _bcheck(lib().llb_batch_get_config(self._b, ctypes.byref(a), ctypes.byref(b)), self._b)
+        return a.value, b.value
+
+    def tune(self, trial_steps: int = 32):
+        by, spl, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        _bcheck(lib().llb_batch_tune(self._b, trial_steps, ctypes.byref(by), ctypes.byref(spl), ctypes.byref(ms)),
+                self._b)
+        return by.value, spl.value, ms.value
+
+    @property
+    def t(self) -> int:
+        s = ctypes.c_int64()
+        _bcheck(lib().llb_batch_get_step(self._b, ctypes.byref(s)), self._b)
+        return s.value
+
+    def synchronize(self):
+        _bcheck(lib().llb_batch_synchronize(self._b), self._b)
+
+    def record(self, slot: int):
+        _bcheck(lib().llb_batch_event_record(self._b, slot), self._b)
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = ctypes.c_float()
+        _bcheck(lib().llb_batch_event_elapsed_ms(self._b, a, b, ctypes.byref(ms)), self._b)
+        return float(ms.value)
+
+    def info(self):
+        n, nodes, by = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _bcheck(lib().llb_batch_info(self._b, ctypes.byref(n), ctypes.byref(nodes), ctypes.byref(by)), self._b)
+        return n.value, nodes.value, by.value

@@ -87,3 +87,62 @@ def parabolic_u(i: int, umax: float, i0: int, i1: int) -> float:
     H = float(i1 - i0 + 1)
     yy = float(i - i0) + 0.5
     return 4.0 * umax * yy * (H - yy) / (H * H)
+
+
+def channel_discs_types(R: int, C: int, n_discs: int, rng: np.random.Generator) -> np.ndarray:
+    """Channel with n_discs non-overlapping random discs (radius 3..max(3, min(R, C) // 8),
+    kept one node clear of each other and two nodes clear of walls, inlet and outlet)."""
+    t = channel_types(R, C)
+    solid = np.zeros((R, C), dtype=bool)
+    rmax = max(3, min(R, C) // 8)
+    placed, tries = 0, 0
+    ii, jj = np.mgrid[0:R, 0:C]
+    while placed < n_discs and tries < 200 * max(n_discs, 1):
+        tries += 1
+        r = int(rng.integers(3, rmax + 1))
+        ci, cj = int(rng.integers(0, R)), int(rng.integers(0, C))
+        lo = r + 3
+        if ci < lo or ci > R - 1 - lo or cj < lo or cj > C - 1 - lo:
+            continue
+        grown = (ii - ci) ** 2 + (jj - cj) ** 2 <= (r + 1) ** 2
+        if solid[grown].any():
+            continue
+        solid[(ii - ci) ** 2 + (jj - cj) ** 2 <= r * r] = True
+        placed += 1
+    t[solid] = OBSTACLE
+    return t
+
+
+def batch_problems(n: int = 256, seed: int = 20261204, max_nx: int = 1024):
+    """Config 4: n independent problems.  nx (columns) uniform in {64, 96, ...,
+    max_nx}, aspect ratio a uniform in [1, 4], ny = round(nx * a) rows; half
+    lid-driven cavities (lid u_x uniform in [0.02, 0.1]), half channels with 0-8
+    random discs (Zou-He inlet u_x uniform in [0.02, 0.1], Zou-He pressure outlet
+    rho = 1); tau uniform in [0.55, 1.5]; BGK or TRT (magic parameter 1/4) with
+    probability 1/2 each.  numpy PCG64 with a fixed seed.  Each problem is a dict
+    with `types` generated lazily by `make_types()`."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = np.arange(64, max_nx + 1, 32)
+    out = []
+    for q in range(n):
+        nx = int(rng.choice(sizes))
+        a = float(rng.uniform(1.0, 4.0))
+        ny = int(round(nx * a))
+        cavity = q % 2 == 0
+        u = float(rng.uniform(0.02, 0.1))
+        tau = float(rng.uniform(0.55, 1.5))
+        trt = bool(rng.integers(0, 2))
+        n_discs = 0 if cavity else int(rng.integers(0, 9))
+        disc_seed = int(rng.integers(0, 2**31))
+        tau_odd = 0.25 * (1.0 / (tau - 0.5)) + 0.5
+        def make(ny=ny, nx=nx, cavity=cavity, n_discs=n_discs, disc_seed=disc_seed):
+            if cavity:
+                t = np.zeros((ny, nx), dtype=np.uint8)
+                t[0, :] = t[-1, :] = t[:, 0] = t[:, -1] = BOUNDARY
+                t[0, 1:-1] = INLET
+                return t
+            return channel_discs_types(ny, nx, n_discs, np.random.Generator(np.random.PCG64(disc_seed)))
+        out.append(dict(rows=ny, cols=nx, kind="cavity" if cavity else "channel", u=u, tau=tau, trt=trt,
+                        tau_odd=tau_odd, n_discs=n_discs, make_types=make,
+                        outlet_bc=0 if cavity else 2))
+    return out
