@@ -23,7 +23,11 @@
 using namespace llb;
 
 namespace {
-constexpr int BATCH_GRAPH_STEPS = 32;
+constexpr int BATCH_GRAPH_STEPS = 32;  // even: a replay keeps every lattice's buffer parity
+// Lattices of at least this many nodes fill the GPU on their own: they are
+// stepped by their own launch of their default kernel (TMA pipeline or one
+// thread per node) inside the batch step instead of through the work list.
+constexpr int64_t SOLO_MIN_NODES = 1 << 20;
 }
 
 struct llb_batch {
@@ -34,6 +38,7 @@ struct llb_batch {
     std::vector<llb_handle> slot;        // nullptr: free slot
     std::vector<BatchLattice> desc;      // per slot
     std::vector<int> order;              // active slots in descriptor order
+    std::vector<int> solo;               // slots stepped by their own launches
     BatchLattice* d_desc = nullptr;
     int desc_cap = 0;
     int2* d_items = nullptr;
@@ -46,7 +51,7 @@ struct llb_batch {
     int block_y = 4;
     int spl = 1;                         // steps per launch
     bool dirty = true;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by parity of the batch step
     cudaEvent_t ev[8] = {};
     std::string err;
 };
@@ -67,9 +72,9 @@ int bfail(llb_batch_handle b, int code, const std::string& m) {
     } while (0)
 
 void drop_graph(llb_batch_handle b) {
-    if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
+    for (auto& g : b->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
     }
 }
 
@@ -100,6 +105,7 @@ int rebuild(llb_batch_handle b) {
     if (!b->dirty) return LLB_OK;
     drop_graph(b);
     b->order.clear();
+    b->solo.clear();
     std::vector<BatchLattice> dev;
     std::vector<int2> items;
     for (int s = 0; s < static_cast<int>(b->slot.size()); ++s) {
@@ -108,6 +114,10 @@ int rebuild(llb_batch_handle b) {
         b->order.push_back(s);
         dev.push_back(b->desc[s]);
         const BatchLattice& d = b->desc[s];
+        if (b->slot[s]->R * b->slot[s]->C >= SOLO_MIN_NODES) {
+            b->solo.push_back(s);
+            continue;
+        }
         const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
         for (int t = 0; t < d.nti * ntj; ++t) items.push_back(make_int2(idx, t));
     }
@@ -157,53 +167,76 @@ int set_base(llb_batch_handle b) {
     return LLB_OK;
 }
 
+// Own launches of the solo lattices for batch step b->step + soff (the step
+// base on the device holds b->step).
+int launch_solo(llb_batch_handle b, long long soff) {
+    for (int s : b->solo) {
+        const BatchLattice& d = b->desc[s];
+        const long long delta = b->step + soff - d.s0;
+        const int rc = handle_launch_step(b->slot[s], d.cur0 ^ static_cast<int>(delta & 1), b->d_sbase,
+                                          soff + d.t0 - d.s0);
+        if (rc != LLB_OK) return bfail(b, rc, std::string("solo lattice: ") + llb_last_error(b->slot[s]));
+    }
+    return LLB_OK;
+}
+
+// Every lattice one step: the work-list kernel and the solo launches.
+int launch_one_step(llb_batch_handle b, long long soff) {
+    if (b->n_items > 0) {
+        cudaError_t e = launch_batch_step(b->storage, launch_desc(b, soff, 1));
+        if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
+    }
+    return launch_solo(b, soff);
+}
+
 int launch_steps(llb_batch_handle b, int32_t nsteps) {
     int rc;
-    if (b->n_items == 0) {
+    if (b->n_items == 0 && b->solo.empty()) {
         b->step += nsteps;
         return LLB_OK;
     }
-    if (b->spl > 1) {
-        // cooperative launches of spl steps each, then the remainder one by one
+    if (b->spl > 1 && b->n_items > 0) {
+        // cooperative launches of spl steps each for the work list, solo
+        // lattices step by step beside them
         while (nsteps > 0) {
             const int k = std::min<int>(nsteps, b->spl);
             if ((rc = set_base(b))) return rc;
             cudaError_t e = launch_batch_step(b->storage, launch_desc(b, 0, k));
             if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
+            for (int s = 0; s < k; ++s)
+                if ((rc = launch_solo(b, s))) return rc;
             b->step += k;
             nsteps -= k;
         }
         return LLB_OK;
     }
     if (nsteps >= BATCH_GRAPH_STEPS) {
-        if (!b->graph) {
+        cudaGraphExec_t& gx = b->graph[b->step & 1];
+        if (!gx) {
             cudaGraph_t g = nullptr;
             LLB_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            cudaError_t le = cudaSuccess;
-            for (int s = 0; s < BATCH_GRAPH_STEPS && le == cudaSuccess; ++s)
-                le = launch_batch_step(b->storage, launch_desc(b, s, 1));
+            int lr = LLB_OK;
+            for (int s = 0; s < BATCH_GRAPH_STEPS && lr == LLB_OK; ++s) lr = launch_one_step(b, s);
             cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
-            if (le != cudaSuccess || ee != cudaSuccess) {
+            if (lr != LLB_OK || ee != cudaSuccess) {
                 if (g) cudaGraphDestroy(g);
-                return bfail(b, LLB_E_CUDA, "capture of the batched step graph failed");
+                return lr != LLB_OK ? lr : bfail(b, LLB_E_CUDA, "capture of the batched step graph failed");
             }
-            cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaError_t ie = cudaGraphInstantiate(&gx, g, 0);
             cudaGraphDestroy(g);
             if (ie != cudaSuccess) return bfail(b, LLB_E_CUDA, "cudaGraphInstantiate (batch)");
         }
         while (nsteps >= BATCH_GRAPH_STEPS) {
             if ((rc = set_base(b))) return rc;
-            LLB_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
+            LLB_BCUDA(b, cudaGraphLaunch(gx, b->stream));
             b->step += BATCH_GRAPH_STEPS;
             nsteps -= BATCH_GRAPH_STEPS;
         }
     }
     if (nsteps > 0) {
         if ((rc = set_base(b))) return rc;
-        for (int s = 0; s < nsteps; ++s) {
-            cudaError_t e = launch_batch_step(b->storage, launch_desc(b, s, 1));
-            if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
-        }
+        for (int s = 0; s < nsteps; ++s)
+            if ((rc = launch_one_step(b, s))) return rc;
         b->step += nsteps;
     }
     return LLB_OK;
@@ -271,7 +304,6 @@ int llb_batch_add(llb_batch_handle b, const llb_desc* desc, const double* open_v
     cudaStreamDestroy(h->stream);
     h->stream = b->stream;
     h->own_stream = false;
-    h->tma_cfg = -1;
     if (open_values && rows > 0 && (rc = llb_set_open_values(h, 0, rows, open_values)) != LLB_OK) {
         llb_destroy(h);
         return bfail(b, rc, "boundary values rejected");

@@ -62,30 +62,35 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, uns
     return ok_sh != 0;
 }
 
+// One tile of one lattice.  The descriptor fields are read once into
+// registers (the stores below cannot alias them).
 template <class M>
-__device__ __forceinline__ void batch_tile(const BatchLattice& L, int tile, long long s) {
+__device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, int tile, long long s) {
     using T = typename M::T;
-    const long long d = s - L.s0;
-    const int cur = L.cur0 ^ static_cast<int>(d & 1);
-    const long long t = L.t0 + d;
-    const T* __restrict__ fin = static_cast<const T*>(L.f[cur]);
-    T* __restrict__ fout = static_cast<T*>(L.f[cur ^ 1]);
-    const Geometry& g = L.g;
-    const int i = (tile % L.nti) * BX + threadIdx.x;
-    const int j = (tile / L.nti) * blockDim.y + threadIdx.y;
+    const long long d = s - Lp->s0;
+    const int cur = Lp->cur0 ^ static_cast<int>(d & 1);
+    const long long t = Lp->t0 + d;
+    const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
+    T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
+    const Geometry g = Lp->g;
+    const int nti = Lp->nti;
+    unsigned* const flags = Lp->flags;
+    const int i = (tile % nti) * BX + threadIdx.x;
+    const int j = (tile / nti) * blockDim.y + threadIdx.y;
     const bool inside = i < g.rows && j < g.cols;
     const long long node = static_cast<long long>(j) * g.ld + i;
     const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
     const uint8_t cls = mask_class(m);
     const bool write_sector = sector_has_active<M>(class_active(cls));
+    const bool warp_plain = __all_sync(0xffffffffu, !(inside && class_active(cls)) || (m & MASK_PLAIN));
     bool bad = false;
     if (inside && class_active(cls)) {
         typename M::R f[9];
-        pull<M>(g, fin, i, j, node, m, f);
+        pull<M>(g, fin, i, j, node, m, warp_plain, f);
         double rho, ux, uy;
         typename M::R rr;
         if (cls == CLS_OPEN) {
-            open_node<M>(L.ot, g.open_idx[node], m, t, f, rho, ux, uy);
+            open_node<M>(Lp->ot, g.open_idx[node], m, t, f, rho, ux, uy);
             rr = M::from_f64(rho);
         } else {
             typename M::R r, x, y;
@@ -95,29 +100,33 @@ __device__ __forceinline__ void batch_tile(const BatchLattice& L, int tile, long
             uy = y;
             bad = !isfinite(M::rho_f64(r));
         }
-        if (L.c.model == 0) M::template collide<0>(f, rr, ux, uy, L.c);
-        else M::template collide<1>(f, rr, ux, uy, L.c);
+        if (Lp->c.model == 0) M::template collide<0>(f, rr, ux, uy, Lp->c);
+        else M::template collide<1>(f, rr, ux, uy, Lp->c);
 #pragma unroll
         for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
     } else if (write_sector && j < g.cols && i < g.ld) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
     }
-    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(L.flags, 1u);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
 }
 
 // One launch: `steps` batch steps starting at batch step (*sbase + soff).
 template <class M>
-__global__ void __launch_bounds__(BX* BY) k_batch_step(const BatchLattice* __restrict__ lats,
+__global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __restrict__ lats,
                                                        const int2* __restrict__ items, int n_items,
                                                        const long long* sbase, long long soff, int steps,
                                                        unsigned* bar, unsigned* err) {
     const long long s0 = *sbase + soff;
     for (int st = 0; st < steps; ++st) {
         const long long s = s0 + st;
+        // the next item's entry is loaded while this one is computed
+        int2 it = blockIdx.x < n_items ? items[blockIdx.x] : make_int2(0, 0);
         for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-            const int2 it = items[item];
-            batch_tile<M>(lats[it.x], it.y, s);
+            const int nxt = item + gridDim.x;
+            const int2 it_next = nxt < n_items ? items[nxt] : it;
+            batch_tile<M>(lats + it.x, it.y, s);
+            it = it_next;
         }
         if (st + 1 < steps && !grid_barrier(bar, bar + 1, gridDim.x)) {
             if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(err, BATCH_FLAG_TIMEOUT);
@@ -143,7 +152,7 @@ __global__ void __launch_bounds__(BX* BY) k_macro_now(Geometry g, OpenTable ot, 
     double rho = 1.0, ux = 0.0, uy = 0.0;
     if (class_active(cls)) {
         typename M::R f[9];
-        pull<M>(g, fin, i, j, node, m, f);
+        pull<M>(g, fin, i, j, node, m, false, f);
         if (cls == CLS_OPEN) {
             open_node<M>(ot, g.open_idx[node], m, t, f, rho, ux, uy);
         } else {

@@ -69,6 +69,7 @@ LaunchCtx make_ctx(llb_handle h) {
     x.g.ld = h->ld;
     x.g.plane = h->plane;
     x.g.mask = h->d_mask;
+    x.g.bb = h->d_bb;
     x.g.open_idx = h->d_open_idx;
     x.ot.vals = h->d_open;
     x.ot.n_open = h->n_open;
@@ -90,7 +91,7 @@ void release(llb_handle h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& g : h->graph)
         if (g) cudaGraphExecDestroy(g);
-    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
+    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
                     h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -105,8 +106,8 @@ void release(llb_handle h) {
 // ---------------------------------------------------------------------------
 constexpr uint8_t UNSET = 0xff;
 
-int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vector<int32_t>& open_idx,
-               std::string& why) {
+int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vector<uint8_t>& bb,
+               std::vector<int32_t>& open_idx, int64_t& n_nonplain, std::string& why) {
     const int64_t R = d->rows, C = d->cols;
     std::vector<uint8_t> cls(static_cast<size_t>(R * C), UNSET);
     auto mark = [&](const int64_t* ij, int64_t n, uint8_t c, const char* name) -> bool {
@@ -152,7 +153,9 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
             }
         }
     }
+    n_nonplain = 0;
     mask.assign(static_cast<size_t>(ld) * C, 0);
+    bb.assign(static_cast<size_t>(ld) * C, 0);
     open_idx.assign(static_cast<size_t>(ld) * C, -1);
     auto side_code = [](int32_t bt) { return (bt >= 1 && bt <= 4) ? bt : SIDE_NONE; };
     for (int64_t j = 0; j < C; ++j) {
@@ -162,13 +165,20 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
             if (c == 1) m = CLS_FLUID;
             else if (c == 2) m = CLS_BB;
             else if (c == 3 || c == 4) m = CLS_OPEN;
+            uint8_t b = 0;
             if (active(c)) {
                 bool plain = true;
-                for (int k = 1; k < 9; ++k)
-                    if (!active(at(i - DI(k), j - DJ(k)))) plain = false;
+                for (int k = 1; k < 9; ++k) {
+                    const int64_t si = i - DI(k), sj = j - DJ(k);
+                    const uint8_t s = at(si, sj);
+                    if (!active(s)) plain = false;
+                    if (s == 2) b |= static_cast<uint8_t>(1u << (k - 1));
+                }
                 if (plain) m |= MASK_PLAIN;
+                else ++n_nonplain;
             }
             mask[static_cast<size_t>(j * ld + i)] = m;
+            bb[static_cast<size_t>(j * ld + i)] = b;
         }
     }
     auto set_open = [&](const int64_t* ij, const int32_t* side, int64_t n, int bc, int base) {
@@ -351,6 +361,22 @@ int handle_force_context(llb_handle h, LaunchCtx* ctx, const void** fin, double*
     return LLB_OK;
 }
 int handle_fail(llb_handle h, int code, const char* msg) { return fail(h, code, msg); }
+int handle_launch_step(llb_handle h, int cur, const long long* tbase, long long t_off) {
+    LaunchCtx x = make_ctx(h);
+    x.ss.tbase = tbase;
+    x.ss.t_off = t_off;
+    cudaError_t e;
+    if (h->tma_cfg >= 0) {
+        int rc = build_maps(h);
+        if (rc) return rc;
+        const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
+        const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
+        e = launch_step_tma(h->storage, h->plan, x, &h->pmap[cur], &h->mmap, h->f[cur], h->f[cur ^ 1], grid);
+    } else {
+        e = launch_step(h->storage, x, h->f[cur], h->f[cur ^ 1], false, false);
+    }
+    return e == cudaSuccess ? LLB_OK : cuda_fail(h, e, "step kernel launch");
+}
 LaunchCtx handle_ctx(llb_handle h) { return make_ctx(h); }
 }  // namespace llb
 
@@ -396,8 +422,6 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     h->plane = static_cast<long long>(h->ld) * d->cols;
     h->n_open = static_cast<int>(n_open);
     h->cap = cap;
-    // default pipeline configuration per storage form (measured on B200, porous 4096^2)
-    h->tma_cfg = d->storage == LLB_STORE_F64 ? 1 : 0;
     if (d->collision == LLB_BGK) {
         h->coll.model = 0;
         h->coll.t = 1.0 / d->tau;  // BGKCollision.hpp:142-143
@@ -409,11 +433,15 @@ int llb_create(const llb_desc* d, llb_handle* out) {
         h->coll.ho = 0.5 * (1.0 / d->tau_odd);
     }
 
-    std::vector<uint8_t> mask;
+    std::vector<uint8_t> mask, bb;
     std::vector<int32_t> open_idx;
     std::string why;
-    int rc = build_mask(d, h->ld, mask, open_idx, why);
+    int rc = build_mask(d, h->ld, mask, bb, open_idx, h->n_nonplain, why);
     if (rc != LLB_OK) { delete h; return fail(nullptr, rc, why); }
+    h->n_active = d->n_fluid + d->n_inlet + d->n_outlet;
+    // default kernel: pipeline configuration 1 (FP64) or 0 (shifted forms), the
+    // fastest measured on the 4096^2 porous channel, or one thread per node
+    h->tma_cfg = prefers_tma(*h) ? (d->storage == LLB_STORE_F64 ? 1 : 0) : -1;
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete h; return fail(nullptr, LLB_E_NODEVICE, "no CUDA device"); }
@@ -428,13 +456,14 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     const size_t pop_bytes = static_cast<size_t>(h->plane) * 9 * h->elem;
     const size_t N = static_cast<size_t>(h->R * h->C);
     if ((rc = dev_alloc(h, &h->f[0], pop_bytes)) || (rc = dev_alloc(h, &h->f[1], pop_bytes)) ||
-        (rc = dev_alloc(h, &h->d_mask, mask.size())) ||
+        (rc = dev_alloc(h, &h->d_mask, mask.size())) || (rc = dev_alloc(h, &h->d_bb, bb.size())) ||
         (rc = dev_alloc(h, &h->d_open_idx, open_idx.size() * sizeof(int32_t))) ||
         (rc = dev_alloc(h, &h->d_open, sizeof(double2) * static_cast<size_t>(std::max<int64_t>(n_open, 1)) * cap)) ||
         (rc = dev_alloc(h, &h->d_rho, sizeof(double) * N)) || (rc = dev_alloc(h, &h->d_u, sizeof(double) * 2 * N)) ||
         (rc = dev_alloc(h, &h->d_step, sizeof(long long))) || (rc = dev_alloc(h, &h->d_flags, sizeof(unsigned))) || (rc = dev_alloc(h, &h->d_red, sizeof(double) * 4)))
         return bail(rc);
     e = cudaMemcpyAsync(h->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_bb, bb.data(), bb.size(), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(h->d_open_idx, open_idx.data(), open_idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)

@@ -29,6 +29,10 @@ namespace llb {
 // from a dead source reads the reference's never-written slot as is.
 constexpr uint8_t CLS_DEAD = 0, CLS_FLUID = 1, CLS_BB = 2, CLS_OPEN = 3;
 constexpr uint8_t MASK_PLAIN = 4;
+// Bounce bits, one byte per node beside the mask (active nodes that are not
+// PLAIN): bit k - 1 set when the source of direction k (1..8), x - c_k, is a
+// wall or obstacle.  Sources outside the lattice (open nodes on the lattice
+// edge only; fluid nodes never lie on it) set no bit.
 constexpr int SIDE_SHIFT = 3, BC_SHIFT = 6;
 constexpr int SIDE_NONE = 0, SIDE_TOP = 1, SIDE_RIGHT = 2, SIDE_BOTTOM = 3, SIDE_LEFT = 4;
 constexpr int BC_ZH_VEL = 0, BC_OPEN = 1, BC_ZH_PRES = 2;
@@ -73,6 +77,7 @@ struct Geometry {
     int ld;             // column stride (elements) of populations / mask / open_idx
     long long plane;    // ld * cols
     const uint8_t* __restrict__ mask;
+    const uint8_t* __restrict__ bb;       // bounce bits
     const int32_t* __restrict__ open_idx;
 };
 

@@ -25,14 +25,28 @@ namespace llb {
 
 constexpr int BX = 32, BY = MAX_BLOCK_Y;  // one warp = 32 rows of one column
 
+// warp_plain: every lane of the warp that pulls has a PLAIN node (a warp vote
+// taken by the caller while the warp is converged; false is always correct).
+// Such warps read straight from the sources; the others take one branch-free
+// path on every lane, where a bounce-back source is only another address
+// (plain lanes skip the bounce-bit load).
 template <class M>
 __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __restrict__ fin, int i, int j,
-                                     long long node, uint8_t m, typename M::R* f) {
+                                     long long node, uint8_t m, bool warp_plain, typename M::R* f) {
     f[0] = M::load(fin + node);
-    if (m & MASK_PLAIN) {
+    if (warp_plain) {
 #pragma unroll
         for (int k = 1; k < 9; ++k) f[k] = M::load(fin + k * g.plane + node - (DJ(k) * g.ld + DI(k)));
+    } else if (i > 0 && j > 0 && i < g.rows - 1 && j < g.cols - 1) {
+        const unsigned b = (m & MASK_PLAIN) ? 0u : g.bb[node];
+#pragma unroll
+        for (int k = 1; k < 9; ++k) {
+            const typename M::T* p = ((b >> (k - 1)) & 1u) ? fin + opp(k) * g.plane + node
+                                                     : fin + k * g.plane + node - (DJ(k) * g.ld + DI(k));
+            f[k] = M::load(p);
+        }
     } else {
+        // open nodes on the lattice edge: sources outside keep their initial value
 #pragma unroll
         for (int k = 1; k < 9; ++k) {
             const int si = i - DI(k), sj = j - DJ(k);
@@ -114,6 +128,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
     const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
     const uint8_t cls = mask_class(m);
     const bool write_sector = sector_has_active<M>(class_active(cls));
+    const bool warp_plain = __all_sync(0xffffffffu, !(inside && class_active(cls)) || (m & MASK_PLAIN));
     if (inside) {
         if (class_active(cls)) {
             typename M::R f[9];
@@ -121,7 +136,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
 #pragma unroll
                 for (int k = 0; k < 9; ++k) f[k] = M::keep(k);
             } else {
-                pull<M>(g, fin, i, j, node, m, f);
+                pull<M>(g, fin, i, j, node, m, warp_plain, f);
             }
             double rho, ux, uy;
             typename M::R rr;
@@ -198,7 +213,7 @@ __global__ void __launch_bounds__(BX* BY) k_finalize(Geometry g, OpenTable ot, c
         return;
     }
     typename M::R f[9];
-    pull<M>(g, fin, i, j, node, m, f);
+    pull<M>(g, fin, i, j, node, m, false, f);
     if (cls == CLS_OPEN && t > 0) {
         const int q = g.open_idx[node];
         const double2 prev = ot.vals[static_cast<long long>((t - 1) % ot.cap) * ot.n_open + q];

@@ -151,3 +151,33 @@ def test_batch_f32s_matches_single_lattice():
             u = b.lattice(slot).compute_macro()[1]
             err = np.sqrt(((u - u1) ** 2).sum() / max((u1 ** 2).sum(), 1e-30))
             assert err <= 1e-6, (prob[0], err)
+
+
+def test_large_lattices_step_by_their_own_kernel_in_the_batch():
+    """Lattices of 2^20 nodes or more run their own default kernel inside the
+    batch step (the TMA pipeline for the porous channel, one thread per node
+    for the cavity), joining at different step parities and crossing graph
+    replays and single steps; every lattice stays bit-exact."""
+    import llalbm_cuda as L
+
+    por = H.classify(H.porous_types(1024, 1024, seed=5))
+    cav = H.classify(H.cavity_types(1024))
+    big_por = ("porous1024", por, H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE), "const:0.02:0", "pressure")
+    big_cav = ("cavity1024", cav, H.Params.trt_magic(0.7), "const:0.05:0", "const:0:0")
+    with L.CudaLattice(por.rows, por.cols, por.fluid, por.wall, por.inlet, por.inlet_side, por.outlet,
+                       por.outlet_side, por.obstacle, por.obstacle_dirs) as g:
+        assert g.pipeline >= 0                      # TMA pipeline by default
+    with L.CudaLattice(cav.rows, cav.cols, cav.fluid, cav.wall, cav.inlet, cav.inlet_side, cav.outlet,
+                       cav.outlet_side, cav.obstacle, cav.obstacle_dirs) as g:
+        assert g.pipeline == -1                     # one thread per node
+    with L.CudaBatch(storage=L.STORE_F64) as b:
+        a = add(b, big_por, 200)
+        s = add(b, PROBLEMS[1], 200)
+        b.step(40)                                  # a, s at 41 (graph + 8 single steps)
+        c = add(b, big_cav, 200)
+        b.step(37)                                  # a, s 78; c 38
+        b.step(33)                                  # odd batch step: the other parity's graph
+        b.synchronize()
+        check_against_oracle(b.lattice(a), big_por, 111)
+        check_against_oracle(b.lattice(s), PROBLEMS[1], 111)
+        check_against_oracle(b.lattice(c), big_cav, 71)
