@@ -209,6 +209,39 @@ def reference_cpu(wl: dict, types: np.ndarray, warmup: int, steps: int) -> dict:
             "seconds": r["seconds"], "steps": steps}
 
 
+def problem_wl(kind: str, collision: int, tau: float, u: float, outlet_bc: int, rows: int) -> dict:
+    """Reference-runner arguments of one batched or served problem."""
+    col = (["--collision", "bgk", "--tau", repr(tau)] if collision == 0 else
+           ["--collision", "trt", "--tau-even", repr(tau), "--magic", "0.25"])
+    if kind == "cavity":
+        bc = ["--inlet", "zh", "--outlet", "zh", "--inlet-u", f"const:{u!r}:0"]
+    elif kind == "cylinder":
+        bc = ["--inlet", "zh", "--outlet", "zhp", "--inlet-u", f"parabolic:0.05:1:{rows - 2}", "--outlet-u",
+              "pressure"]
+    else:
+        bc = ["--inlet", "zh", "--outlet", "zhp" if outlet_bc == 2 else "zh", "--inlet-u", f"const:{u!r}:0",
+              "--outlet-u", "pressure" if outlet_bc == 2 else "const:0:0"]
+    return {"ref_args": col + bc}
+
+
+def reference_sample(items, warmup: int, steps: int) -> dict:
+    """The reference's OpenMP path over a sample of independent problems, one
+    after another (one Lattice per problem): node updates / summed time."""
+    work, secs, names = 0, 0.0, []
+    for wl, types in items:
+        r = reference_cpu(wl, types, warmup, steps)
+        if r is None or "error" in r:
+            return r
+        work += types.shape[0] * types.shape[1] * steps
+        secs += r["seconds"]
+        names.append(f"{types.shape[0]}x{types.shape[1]}")
+        cores = r["cores"]
+    return {"value": work / secs / 1e6, "unit": "MLUPS", "cores": cores, "kind": "reference",
+            "sample": f"LLALBM perform_lbm, OMPPolicy, problems {', '.join(names)} one after another, "
+                      f"{steps} timed steps each after {warmup} warm-up, {cores} threads",
+            "seconds": secs, "steps": steps}
+
+
 def oracle_cpu(wl: dict, types: np.ndarray, steps: int) -> dict:
     """Fallback when the reference could not be compiled: the C restatement."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -442,6 +475,159 @@ def run_batch(a, dist):
     }
 
 
+# ---------------------------------------------------------------------------
+# served solve stream (config 5)
+# ---------------------------------------------------------------------------
+def serve_prepare(L, reqs):
+    """Node lists and boundary values of every request, built before any clock
+    starts (a client holds its lattice description before it submits)."""
+    cache = {}
+    out = []
+    for r in reqs:
+        key = (r["kind"], r["rows"], r["cols"])
+        if key not in cache:
+            n = L.classify(r["make_types"]())
+            cache[key] = (n, len(n["fluid"]) + len(n["inlet"]) + len(n["outlet"]))
+        n, active = cache[key]
+        out.append(dict(req=r, lists=n, active=active, table=W.serve_open_values(r, n)))
+    return out
+
+
+def serve_submit(server, p, steps=None):
+    r, n = p["req"], p["lists"]
+    return server.submit(r["rows"], r["cols"], n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"],
+                         n["outlet_side"], n["obstacle"], n["obstacle_dirs"], steps=steps or r["steps"],
+                         collision=r["collision"], tau=r["tau"], tau_even=r["tau_even"], tau_odd=r["tau_odd"],
+                         outlet_bc=r["outlet_bc"], open_values=p["table"])
+
+
+def serve_stream(L, prepared, arrivals, storage, mode, budget, warmup):
+    """Submits every request at its arrival time (a feeder thread), collects
+    every result (rho and u copied to host memory); latency = done - submitted."""
+    import queue as Q
+
+    with L.CudaServer(storage=storage, mode=mode, budget_bytes=budget, max_chunk_steps=256) as s:
+        small = sorted(prepared, key=lambda p: p["req"]["rows"] * p["req"]["cols"])[:max(warmup, 1)]
+        for p in small:                                   # warm-up: module load, first graphs
+            rid = serve_submit(s, p, steps=200)
+            s.wait(rid, 600)
+            s.result(rid, fields=False)
+        st0 = s.stats()
+        ids = Q.Queue()
+        t_start = time.perf_counter() + 0.02
+
+        def feeder():
+            for q, p in enumerate(prepared):
+                delay = t_start + arrivals[q] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                ids.put((q, serve_submit(s, p)))
+        th = threading.Thread(target=feeder)
+        th.start()
+        times = [None] * len(prepared)
+        peak = 0
+        for _ in prepared:
+            q, rid = ids.get()
+            while True:
+                try:
+                    s.wait(rid, 0.05)
+                    break
+                except L.LLBError as e:
+                    if e.code != -9:
+                        raise
+                    peak = max(peak, s.stats()["bytes_in_use"])
+            rho, u, times[q] = s.result(rid)
+        th.join()
+        st = s.stats()
+    sub = np.array([t[0] for t in times])
+    adm = np.array([t[1] for t in times])
+    done = np.array([t[2] for t in times])
+    lat = done - sub
+    span = float(done.max() - sub.min())
+    work = sum(p["req"]["rows"] * p["req"]["cols"] * p["req"]["steps"] for p in prepared)
+    pct = {f"p{q}": round(float(np.percentile(lat, q)), 4) for q in (50, 95, 99)}
+    busy = float(np.sum(done - adm)) if mode == L.SERVE_SEQUENTIAL else None
+    return {"mlups": work / span / 1e6, "span_s": span, "latency_s": pct,
+            "busy_mlups": None if busy is None else round(work / busy / 1e6, 1),
+            "latency_mean_s": round(float(lat.mean()), 4), "queue_wait_mean_s": round(float((adm - sub).mean()), 4),
+            "node_updates": work, "peak_bytes_in_use": int(peak), "chunks": st["chunks"] - st0["chunks"],
+            "batch_steps": st["batch_steps"] - st0["batch_steps"], "t0": float(sub.min()), "t1": float(done.max())}
+
+
+def run_serve(a, dist):
+    """Config 5: a Poisson stream of requests served by continuous batching
+    (FP32-shifted) and, as the comparison, the same stream through the plain
+    FP64 path one request at a time."""
+    import llalbm_cuda as L
+
+    reqs = W.serve_requests(a.requests)
+    prepared = serve_prepare(L, reqs)
+    budget = 120 * 10**9
+    # capacity: every request of the stream resident in one batch, device-timed steps
+    with L.CudaBatch(storage=L.STORE_F32S, device=dist.local) as b:
+        for p in prepared:
+            r, n = p["req"], p["lists"]
+            b.add(r["rows"], r["cols"], n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"],
+                  n["outlet_side"], n["obstacle"], n["obstacle_dirs"], collision=r["collision"], tau=r["tau"],
+                  tau_even=r["tau_even"], tau_odd=r["tau_odd"], outlet_bc=r["outlet_bc"], open_values=p["table"])
+        b.set_config(8, 1)
+        b.step(32)
+        b.synchronize()
+        b.record(0)
+        b.step(128)
+        b.record(1)
+        cap_ms = b.elapsed_ms(0, 1)
+    nodes = sum(p["req"]["rows"] * p["req"]["cols"] for p in prepared)
+    cal = {"mlups": nodes * 128 / cap_ms / 1e3}
+    capacity = cal["mlups"] * 1e6
+    mean_work = np.mean([p["req"]["rows"] * p["req"]["cols"] * p["req"]["steps"] for p in prepared])
+    rate = 0.7 * capacity / mean_work
+    arrivals = W.poisson_arrivals(len(prepared), rate)
+    sampler = ClockSampler(dist.local)
+    batched = serve_stream(L, prepared, arrivals, L.STORE_F32S, L.SERVE_BATCHED, budget, a.warmup)
+    clocks = sampler.summary(batched["t0"] - time.monotonic() + time.perf_counter(),
+                             batched["t1"] - time.monotonic() + time.perf_counter())
+    plain = serve_stream(L, prepared, arrivals, L.STORE_F64, L.SERVE_SEQUENTIAL, budget, a.warmup)
+    sampler.stop()
+    peak = (json.load(open(PEAKS_FILE)).get("hbm_gbs") if os.path.exists(PEAKS_FILE) else None) or FALLBACK_HBM_GBS
+    bytes_total = sum((18 * 4 * p["active"] + p["req"]["rows"] * p["req"]["cols"]) * p["req"]["steps"]
+                      for p in prepared)
+    gbs = bytes_total / batched["span_s"] / 1e9
+    h2d = sum(16 * (len(p["lists"]["fluid"]) + len(p["lists"]["wall"]) + len(p["lists"]["inlet"]) +
+                    len(p["lists"]["outlet"]) + len(p["lists"]["obstacle"])) + p["table"].nbytes for p in prepared)
+    d2h = sum(24 * p["req"]["rows"] * p["req"]["cols"] for p in prepared)
+    strip = lambda d: {k: v for k, v in d.items() if k not in ("t0", "t1")}
+    return {
+        "metric": METRIC, "value": round(batched["mlups"], 1), "unit": "MLUPS", "n_gpus": dist.world,
+        "steps": len(prepared), "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (shifted storage)", "data": "synthetic",
+        "config": {"workload": "serve", "requests": len(prepared),
+                   "description": "Poisson arrivals; side log-uniform 128..2048 (multiple of 16); steps uniform "
+                                  "1k..20k; cavity / cylinder channel / porous channel 1:1:1; FP32-shifted; "
+                                  "120 GB admission budget; rate 0.7 x capacity measured on a burst",
+                   "rate_per_s": round(rate, 4), "capacity_mlups": round(cal["mlups"], 1),
+                   "capacity_is": "all requests of the stream resident in one FP32-shifted batch, 128 device-timed "
+                                  "batch steps",
+                   "value_is": "node updates of all requests / (last done - first submitted), wall clock through "
+                               "the C ABI server with host buffers in and out",
+                   "steps_field": "number of requests"},
+        "serve": {"batched_f32s": strip(batched), "plain_f64_sequential": strip(plain),
+                  "mlups_ratio": round(batched["mlups"] / plain["mlups"], 3),
+                  "capacity_ratio": round(cal["mlups"] / plain["busy_mlups"], 3),
+                  "capacity_ratio_is": "batched FP32-shifted capacity / plain FP64 throughput while busy "
+                                       "(node updates / summed per-request service time)"},
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(gbs / peak, 4), "traffic": None,
+                     "note": "algorithmic bytes of all requests over the stream's wall-clock span (offered load "
+                             "0.7 of capacity)"},
+        "e2e": {"value": round(batched["mlups"], 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d / len(prepared)),
+                "d2h_bytes_per_step": int(d2h / len(prepared)),
+                "path": "llb_server_submit (node lists + boundary values from host memory) ... llb_server_result "
+                        "(rho, u to host memory); per request"},
+        "gpu_launches": batched["batch_steps"] + 4 * len(prepared), "clocks": clocks,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,7 +635,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="porous4096",
-                    choices=("porous4096", "cylinder1024x256", "cavity129", "batch256"))
+                    choices=("porous4096", "cylinder1024x256", "cavity129", "batch256", "serve"))
+    ap.add_argument("--requests", type=int, default=96, help="requests in the served stream (workload serve)")
     ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous workload")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -460,12 +647,32 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return
-        wl = workload(a.workload, a.size)
-        types = wl["types"]()
-        w, k = min(a.warmup, 2), max(1, min(a.steps, 5 if a.workload == "porous4096" else 200))
-        r = reference_cpu(wl, types, w, k)
-        if r is None:
-            r = oracle_cpu(wl, types, k)
+        w = min(a.warmup, 2)
+        if a.workload in ("batch256", "serve"):
+            # a sample of the independent problems, each through its own Lattice
+            if a.workload == "batch256":
+                probs = W.batch_problems()[:6]
+                items = [(problem_wl(p["kind"], int(p["trt"]), p["tau"], p["u"], p["outlet_bc"], p["rows"]),
+                          p["make_types"]()) for p in probs]
+                desc = "256 uneven problems (sample of 6)"
+            else:
+                reqs = W.serve_requests(a.requests)[:6]
+                items = [(problem_wl(r["kind"], r["collision"], r["tau_even"], r["lid"] or 0.02, r["outlet_bc"],
+                                     r["rows"]), r["make_types"]()) for r in reqs]
+                desc = "served request stream (sample of 6 requests)"
+            k = max(1, min(a.steps, 20))
+            r = reference_sample(items, w, k)
+            wl = {"name": a.workload, "desc": desc}
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_runner_fast was not built"}))
+                return
+        else:
+            wl = workload(a.workload, a.size)
+            types = wl["types"]()
+            k = max(1, min(a.steps, 5 if a.workload == "porous4096" else 200))
+            r = reference_cpu(wl, types, w, k)
+            if r is None:
+                r = oracle_cpu(wl, types, k)
         if "error" in r:
             print(json.dumps({"impl": "reference", "unavailable": "reference runner failed: " + r["error"][-200:]}))
             return
@@ -480,8 +687,8 @@ def main():
         return
 
     dist = Dist(a.gpus)
-    if a.workload == "batch256":
-        line = run_batch(a, dist)
+    if a.workload in ("batch256", "serve"):
+        line = run_batch(a, dist) if a.workload == "batch256" else run_serve(a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)
         dist.close()

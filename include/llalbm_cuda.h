@@ -235,6 +235,52 @@ int llb_batch_event_elapsed_ms(llb_batch_handle b, int32_t slot_begin, int32_t s
 int llb_batch_info(llb_batch_handle b, int64_t* lattices, int64_t* nodes, int64_t* device_bytes);
 const char* llb_batch_last_error(llb_batch_handle b);
 
+/* ---- solve server -------------------------------------------------------- */
+/* A request loop over a batch; no counterpart in the reference (one Lattice
+   per process, driven by its own main()).  Requests -- a lattice description,
+   its boundary values for steps 0..rows-1 and a step count -- are submitted
+   from any thread and queued; one worker thread admits them first come, first
+   served while the device bytes of the admitted lattices fit budget_bytes,
+   keeps their state resident and advances them (batched mode: together, one
+   batch, in chunks of at most max_chunk_steps, admitting arrivals between
+   chunks while the previous chunk runs; sequential mode: one at a time
+   through the plain single-lattice path).  A request of `steps` steps (>= 2)
+   ends with the state the reference's Lattice holds after perform_lbm(steps)
+   and returns that call's rho and u: steps - 1 collisions and the macroscopic
+   fields of the last step (llb_compute_macro).  The lattice's storage, device
+   and pattern come from the server, not from the description.  Timestamps are
+   seconds on a monotonic clock (llb_server_counters.clock_s is "now"). */
+#define LLB_SERVE_BATCHED 0
+#define LLB_SERVE_SEQUENTIAL 1
+#define LLB_REQ_QUEUED 0
+#define LLB_REQ_RUNNING 1
+#define LLB_REQ_DONE 2
+#define LLB_REQ_FAILED 3
+typedef struct llb_server* llb_server_handle;
+/* completed / failed requests, lattice-node updates of the completed ones,
+   requests queued and running now, device bytes charged, chunks launched and
+   the batch steps they ran (one persistent launch each), the clock now. */
+typedef struct {
+    int64_t completed, failed, node_steps, queued, running, bytes_in_use, chunks, batch_steps;
+    double clock_s;
+} llb_server_counters;
+int llb_server_create(int32_t device, int32_t storage, int32_t mode, int64_t budget_bytes, int32_t max_chunk_steps,
+                      llb_server_handle* out);
+/* Stops the worker after the running requests finish; queued ones fail. */
+int llb_server_destroy(llb_server_handle s);
+/* LLB_E_NOMEM if the lattice alone exceeds the budget.  The description's
+   arrays and open_values are copied before the call returns. */
+int llb_server_submit(llb_server_handle s, const llb_desc* desc, const double* open_values, int32_t rows,
+                      int64_t steps, int64_t* request_id);
+int llb_server_poll(llb_server_handle s, int64_t request_id, int32_t* state);
+/* LLB_OK when done, LLB_E_TIMEOUT after timeout_s, LLB_E_CUDA if it failed. */
+int llb_server_wait(llb_server_handle s, int64_t request_id, double timeout_s);
+/* Copies rho (R*C) and u (R*C*2) (either may be NULL) and times = {submitted,
+   admitted, done}; releases the request. */
+int llb_server_result(llb_server_handle s, int64_t request_id, double* rho, double* u, double times[3]);
+int llb_server_stats(llb_server_handle s, llb_server_counters* out);
+const char* llb_server_last_error(llb_server_handle s);
+
 /* ---- synchronisation, timing, errors ------------------------------------ */
 
 int llb_synchronize(llb_handle h);

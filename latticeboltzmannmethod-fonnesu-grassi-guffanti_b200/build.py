@@ -30,6 +30,7 @@ SOURCES = {
     "llb_capi.cu": [],
     "llb_noalloc.cu": [],
     "llb_batch.cu": [],
+    "llb_server.cpp": [],
     "llb_classify.cpp": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [

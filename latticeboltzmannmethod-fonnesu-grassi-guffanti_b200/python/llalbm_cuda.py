@@ -29,6 +29,8 @@ STORE_F64, STORE_F32S, STORE_F16S = 0, 1, 2
 PATTERN_AB, PATTERN_AA = 0, 1
 BC_ZH_VELOCITY, BC_OPEN, BC_ZH_PRESSURE = 0, 1, 2
 STEP_MACRO = 1
+SERVE_BATCHED, SERVE_SEQUENTIAL = 0, 1
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 STORAGE_BYTES = {STORE_F64: 8, STORE_F32S: 4, STORE_F16S: 2}
 
 
@@ -115,6 +117,16 @@ SIGNATURES = {
                        ctypes.POINTER(ctypes.c_int64)],
     "llb_batch_last_error": [_H],
     "llb_device_bytes": [_H, ctypes.POINTER(ctypes.c_int64)],
+    "llb_server_create": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                          ctypes.POINTER(_H)],
+    "llb_server_destroy": [_H],
+    "llb_server_submit": [_H, ctypes.POINTER(_Desc), _P, ctypes.c_int32, ctypes.c_int64,
+                          ctypes.POINTER(ctypes.c_int64)],
+    "llb_server_poll": [_H, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)],
+    "llb_server_wait": [_H, ctypes.c_int64, ctypes.c_double],
+    "llb_server_result": [_H, ctypes.c_int64, _P, _P, _P],
+    "llb_server_stats": [_H, _P],
+    "llb_server_last_error": [_H],
 }
 
 
@@ -455,3 +467,95 @@ class CudaBatch:
         n, nodes, by = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _bcheck(lib().llb_batch_info(self._b, ctypes.byref(n), ctypes.byref(nodes), ctypes.byref(by)), self._b)
         return n.value, nodes.value, by.value
+
+
+class _ServerCounters(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("completed", "failed", "node_steps", "queued", "running",
+                                             "bytes_in_use", "chunks", "batch_steps")] + [("clock_s", ctypes.c_double)]
+
+
+def _scheck(rc: int, s):
+    if rc != LLB_OK:
+        msg = lib().llb_server_last_error(s) if s else b""
+        raise LLBError(rc, msg.decode() if msg else "")
+
+
+class CudaServer:
+    """Solve server: requests (lattice, boundary values, step count) submitted
+    from any thread are admitted under a device-memory budget and served by a
+    native worker thread -- batched (continuous batching over one CudaBatch) or
+    sequential (the plain single-lattice path, one request at a time).
+
+    A request of `steps` steps returns the rho and u that the reference's
+    Lattice holds after perform_lbm(steps)."""
+
+    def __init__(self, storage: int = STORE_F32S, mode: int = SERVE_BATCHED, budget_bytes: int = 120 * 10**9,
+                 max_chunk_steps: int = 256, device: int = 0):
+        s = ctypes.c_void_p()
+        _check(lib().llb_server_create(device, storage, mode, int(budget_bytes), max_chunk_steps, ctypes.byref(s)))
+        self._s, self.storage, self.mode, self.device = s, storage, mode, device
+        self._shape = {}
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().llb_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs=None,
+               *, steps: int, collision=BGK, tau=0.6, tau_even=0.6, tau_odd=0.6, inlet_bc=BC_ZH_VELOCITY,
+               outlet_bc=BC_ZH_VELOCITY, open_values=None) -> int:
+        """Queues one request; returns its id.  open_values: [rows][n_open][2]
+        for steps 0.. (the last row repeats for later steps)."""
+        vals = None if open_values is None else np.ascontiguousarray(open_values, dtype=np.float64)
+        nrows = 0 if vals is None else vals.reshape(-1, len(inlet) + len(outlet), 2).shape[0]
+        d, keep = _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs,
+                        collision=collision, tau=tau, tau_even=tau_even, tau_odd=tau_odd, inlet_bc=inlet_bc,
+                        outlet_bc=outlet_bc, storage=self.storage, pattern=PATTERN_AB, device=self.device,
+                        open_table_rows=max(nrows, 1))
+        rid = ctypes.c_int64()
+        _scheck(lib().llb_server_submit(self._s, ctypes.byref(d), _ptr(vals), nrows, int(steps), ctypes.byref(rid)),
+                self._s)
+        self._shape[rid.value] = (int(rows), int(cols))
+        return rid.value
+
+    def submit_types(self, types, **kw) -> int:
+        n = classify(types)
+        R, C = types.shape
+        return self.submit(R, C, n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"], n["outlet_side"],
+                           n["obstacle"], n["obstacle_dirs"], **kw)
+
+    def state(self, rid: int) -> int:
+        st = ctypes.c_int32()
+        _scheck(lib().llb_server_poll(self._s, rid, ctypes.byref(st)), self._s)
+        return st.value
+
+    def wait(self, rid: int, timeout_s: float = 600.0):
+        _scheck(lib().llb_server_wait(self._s, rid, float(timeout_s)), self._s)
+
+    def result(self, rid: int, fields: bool = True):
+        """(rho, u, times): rho[j, i], u[c, j, i] (None unless fields) and
+        times = (submitted, admitted, done) in seconds; releases the request."""
+        R, C = self._shape[rid]
+        rho = np.empty((C, R)) if fields else None
+        u = np.empty((2, C, R)) if fields else None
+        times = np.zeros(3)
+        _scheck(lib().llb_server_result(self._s, rid, _ptr(rho), _ptr(u), _ptr(times)), self._s)
+        del self._shape[rid]
+        return rho, u, tuple(float(x) for x in times)
+
+    def stats(self) -> dict:
+        c = _ServerCounters()
+        _scheck(lib().llb_server_stats(self._s, ctypes.byref(c)), self._s)
+        return {k: getattr(c, k) for k, _ in c._fields_}

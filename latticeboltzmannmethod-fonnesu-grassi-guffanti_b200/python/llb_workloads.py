@@ -146,3 +146,75 @@ def batch_problems(n: int = 256, seed: int = 20261204, max_nx: int = 1024):
                         tau_odd=tau_odd, n_discs=n_discs, make_types=make,
                         outlet_bc=0 if cavity else 2))
     return out
+
+
+def serve_requests(n: int = 96, seed: int = 20261205, side_min: int = 128, side_max: int = 2048,
+                   steps_min: int = 1000, steps_max: int = 20000):
+    """Config 5 request stream (without arrival times): lattice side s
+    log-uniform in [side_min, side_max] (rounded to a multiple of 16), steps
+    uniform in [steps_min, steps_max], kind uniform over the three single-lattice
+    cases:
+
+      cavity    s x s lid-driven cavity, BGK tau 0.884, lid u = (0.1, 0)
+      cylinder  (s/4) x s channel (at least 32 rows), TRT magic 1/4, parabolic
+                Zou-He inlet u_max 0.05, Zou-He pressure outlet rho 1, staircase
+                cylinder of radius 20/256 of the height at (200/1024, 131/256)
+                of the channel, tau from Re 200: nu = 0.05 * 2r / 200
+      porous    s x s random porous channel (discs r 3..12, 30 % solid, seed
+                from the side), BGK tau 0.8, Zou-He inlet u 0.02, Zou-He
+                pressure outlet rho 1
+
+    numpy PCG64 with a fixed seed.  Each request is a dict with `make_types()`
+    and `open_values(lists)` (one row of boundary values, repeated for every
+    step)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for q in range(n):
+        side = int(round(np.exp(rng.uniform(np.log(side_min), np.log(side_max))) / 16.0)) * 16
+        side = min(max(side, side_min), side_max)
+        steps = int(rng.integers(steps_min, steps_max + 1))
+        kind = ("cavity", "cylinder", "porous")[int(rng.integers(0, 3))]
+        if kind == "cavity":
+            R, C = side, side
+            req = dict(collision=0, tau=0.884, tau_even=0.884, tau_odd=0.884, outlet_bc=0)
+            make = (lambda s=side: cavity_types(s))
+            lid = 0.1
+        elif kind == "cylinder":
+            R, C = max(32, side // 4), side
+            r = max(3, int(round(20.0 * R / 256.0)))
+            tau = 3.0 * (0.05 * 2 * r / 200.0) + 0.5
+            req = dict(collision=1, tau=tau, tau_even=tau, tau_odd=0.25 / (tau - 0.5) + 0.5, outlet_bc=2)
+            x0, y0 = int(round(200.0 * C / 1024.0)), int(round(131.0 * R / 256.0))
+            make = (lambda R=R, C=C, x0=x0, y0=y0, r=r: cylinder_types(R, C, x0, y0, r))
+            lid = None
+        else:
+            R, C = side, side
+            req = dict(collision=0, tau=0.8, tau_even=0.8, tau_odd=0.8, outlet_bc=2)
+            make = (lambda s=side: porous_types(s, s, seed=20261203 + s))
+            lid = None
+        req.update(kind=kind, rows=R, cols=C, steps=steps, make_types=make, lid=lid)
+        out.append(req)
+    return out
+
+
+def serve_open_values(req: dict, lists: dict) -> np.ndarray:
+    """One row of boundary values for a config-5 request (inlets, then outlets)."""
+    ni, no = len(lists["inlet"]), len(lists["outlet"])
+    t = np.zeros((1, ni + no, 2))
+    if req["kind"] == "cavity":
+        t[0, :ni, 0] = req["lid"]
+    elif req["kind"] == "cylinder":
+        R = req["rows"]
+        for q, (i, _) in enumerate(lists["inlet"]):
+            t[0, q, 0] = parabolic_u(int(i), 0.05, 1, R - 2)
+        t[0, ni:] = (1.0, 0.0)
+    else:
+        t[0, :ni, 0] = 0.02
+        t[0, ni:] = (1.0, 0.0)
+    return t
+
+
+def poisson_arrivals(n: int, rate_per_s: float, seed: int = 20261206) -> np.ndarray:
+    """Arrival times (seconds from 0) of a Poisson process: exponential gaps."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.cumsum(rng.exponential(1.0 / rate_per_s, size=n))

@@ -123,3 +123,23 @@ def test_create_without_gpu_reports_no_device():
     with pytest.raises(L.LLBError) as e:
         L.CudaLattice(**_desc_kw(lists))
     assert e.value.code in (-5, -4)
+
+
+def test_server_validates_arguments_and_device():
+    import llalbm_cuda as L
+
+    with pytest.raises(L.LLBError) as e:
+        L.CudaServer(budget_bytes=0)
+    assert e.value.code == -1
+    with pytest.raises(L.LLBError) as e:
+        L.CudaServer(mode=5)
+    assert e.value.code == -1
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return
+    except ImportError:
+        pass
+    with pytest.raises(L.LLBError) as e:
+        L.CudaServer()
+    assert e.value.code == -5
