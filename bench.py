@@ -299,6 +299,35 @@ def time_form(L, wl, nodes, R, C, storage, device, warmup, steps, dist, sampler=
     return g, ms, (t0, t1), u
 
 
+def drag_lift(L, wl, nodes, R, C, device, steps, every=100):
+    """Drag and lift of every storage form, sampled every `every` steps with
+    the compensated FP64 reduction, against the FP64 run: drag relative to
+    itself, lift relative to its amplitude, over the second half of the run
+    (the developed street)."""
+    hist = {}
+    for storage in (0, 1, 2):
+        g = make_lattice(L, wl, nodes, R, C, storage, device)
+        g.init()
+        g.set_force_points(nodes["obstacle"], nodes["obstacle_dirs"])
+        h, done = [], 1
+        while done + every <= steps:
+            g.step(every)
+            done += every
+            h.append(g.flow_forces())
+        g.close()
+        hist[storage] = np.array(h)
+    half = len(hist[0]) // 2
+    lift64, drag64 = hist[0][half:, 0], hist[0][half:, 1]
+    out = {"steps": steps, "every": every, "drag_mean_f64": float(drag64.mean()),
+           "lift_amplitude_f64": float(np.abs(lift64).max())}
+    for storage, name in ((1, "f32s"), (2, "f16s")):
+        lift, drag = hist[storage][half:, 0], hist[storage][half:, 1]
+        out[name] = {"drag_mean": float(drag.mean()),
+                     "drag_max_rel_err": float(np.max(np.abs(drag - drag64) / np.abs(drag64))),
+                     "lift_max_err_rel_amplitude": float(np.max(np.abs(lift - lift64)) / np.abs(lift64).max())}
+    return out
+
+
 def run_ours(a, dist):
     import llalbm_cuda as L
 
@@ -357,6 +386,9 @@ def run_ours(a, dist):
     e_s = dist.max(time.perf_counter() - t_e)
     g.close()
     sampler.stop()
+    forces = None
+    if wl["name"] == "cylinder1024x256" and a.force_steps > 0:
+        forces = drag_lift(L, wl, nodes, R, C, dev, a.force_steps)
 
     f64 = forms["f64"]
     peaks = {}
@@ -388,6 +420,8 @@ def run_ours(a, dist):
         "gpu_launches": a.steps,
         "clocks": clocks,
     }
+    if forces:
+        line["drag_lift"] = forces
     return line, wl, types
 
 
@@ -547,7 +581,7 @@ def serve_stream(L, prepared, arrivals, storage, mode, budget, warmup):
     work = sum(p["req"]["rows"] * p["req"]["cols"] * p["req"]["steps"] for p in prepared)
     pct = {f"p{q}": round(float(np.percentile(lat, q)), 4) for q in (50, 95, 99)}
     busy = float(np.sum(done - adm)) if mode == L.SERVE_SEQUENTIAL else None
-    return {"mlups": work / span / 1e6, "span_s": span, "latency_s": pct,
+    return {"mlups": round(work / span / 1e6, 1), "span_s": round(span, 3), "latency_s": pct,
             "busy_mlups": None if busy is None else round(work / busy / 1e6, 1),
             "latency_mean_s": round(float(lat.mean()), 4), "queue_wait_mean_s": round(float((adm - sub).mean()), 4),
             "node_updates": work, "peak_bytes_in_use": int(peak), "chunks": st["chunks"] - st0["chunks"],
@@ -604,7 +638,7 @@ def run_serve(a, dist):
         "config": {"workload": "serve", "requests": len(prepared),
                    "description": "Poisson arrivals; side log-uniform 128..2048 (multiple of 16); steps uniform "
                                   "1k..20k; cavity / cylinder channel / porous channel 1:1:1; FP32-shifted; "
-                                  "120 GB admission budget; rate 0.7 x capacity measured on a burst",
+                                  "120 GB admission budget; arrival rate 0.7 x the measured capacity",
                    "rate_per_s": round(rate, 4), "capacity_mlups": round(cal["mlups"], 1),
                    "capacity_is": "all requests of the stream resident in one FP32-shifted batch, 128 device-timed "
                                   "batch steps",
@@ -640,6 +674,10 @@ def main():
     ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous workload")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="porous workload: skip the batched and served summaries")
+    ap.add_argument("--force-steps", type=int, default=50000,
+                    help="cylinder workload: steps of the drag/lift comparison of the storage forms (0: skip)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -694,6 +732,25 @@ def main():
         dist.close()
         return
     line, wl, types = run_ours(a, dist)
+    if dist.world == 1 and a.workload == "porous4096" and not a.no_extras:
+        # the batched and served FP32-shifted forms beside the plain FP64 path
+        import copy
+        ab = copy.copy(a)
+        ab.steps = min(a.steps, 300)
+        bl = run_batch(ab, dist)
+        line["batched"] = {"workload": "batch256", "mlups_f32s": bl["value"], "plain_f64_mlups": bl["plain_f64"]["mlups"],
+                           "ratio": bl["batched_over_plain_f64"], "roofline_frac": bl["roofline"]["frac"],
+                           "steps": ab.steps, "launch": bl["config"]["launch"]}
+        asv = copy.copy(a)
+        asv.requests = min(a.requests, 64)
+        sl = run_serve(asv, dist)
+        sv = sl["serve"]
+        line["served"] = {"workload": "serve", "requests": asv.requests, "rate_per_s": sl["config"]["rate_per_s"],
+                          "capacity_mlups_f32s": sl["config"]["capacity_mlups"],
+                          "f32s_batched": {k: sv["batched_f32s"][k] for k in ("mlups", "latency_s")},
+                          "f64_plain_sequential": {k: sv["plain_f64_sequential"][k] for k in ("mlups", "busy_mlups",
+                                                                                              "latency_s")},
+                          "mlups_ratio": sv["mlups_ratio"], "capacity_ratio": sv["capacity_ratio"]}
     if dist.rank == 0:
         if dist.world == 1 and not a.no_cpu_baseline:
             cb = reference_cpu(wl, types, 1, 3 if a.workload == "porous4096" else 100)

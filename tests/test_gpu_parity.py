@@ -229,3 +229,38 @@ def test_numerics_flag():
         with pytest.raises(L.LLBError) as e:
             g.check_numerics()
         assert e.value.code == -7
+
+
+def test_cylinder_drag_lift_shifted_f32_within_a_thousandth():
+    """The 1024 x 256 cylinder street (TRT magic 1/4, parabolic inlet u_max
+    0.05, pressure outlet): drag and lift of the FP32-shifted form, sampled
+    every 100 steps with the compensated FP64 reduction once the flow has
+    developed, stay within 0.1 % of the FP64 run (drag relative to itself,
+    lift relative to its amplitude)."""
+    import llalbm_cuda as L
+
+    types = H.cylinder_types()
+    n = L.classify(types)
+    R, C = types.shape
+    ni, no = len(n["inlet"]), len(n["outlet"])
+    tab = np.zeros((1, ni + no, 2))
+    tab[0, :ni, 0] = [H.parabolic_u(int(i), 0.05, 1, R - 2) for i in n["inlet"][:, 0]]
+    tab[0, ni:] = (1.0, 0.0)
+    te = 3.0 * (0.05 * 40 / 200) + 0.5
+    hist = {}
+    for storage in (L.STORE_F64, L.STORE_F32S):
+        with L.CudaLattice(R, C, n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"], n["outlet_side"],
+                           n["obstacle"], n["obstacle_dirs"], collision=L.TRT, tau_even=te,
+                           tau_odd=0.25 / (te - 0.5) + 0.5, outlet_bc=L.BC_ZH_PRESSURE, storage=storage) as g:
+            g.set_open_values(tab)
+            g.init()
+            g.set_force_points(n["obstacle"], n["obstacle_dirs"])
+            h = []
+            for _ in range(160):
+                g.step(100)
+                h.append(g.flow_forces())
+            hist[storage] = np.array(h)[80:]          # steps 8001..16001: the street has formed
+    lift64, drag64 = hist[L.STORE_F64][:, 0], hist[L.STORE_F64][:, 1]
+    lift32, drag32 = hist[L.STORE_F32S][:, 0], hist[L.STORE_F32S][:, 1]
+    assert np.max(np.abs(drag32 - drag64) / np.abs(drag64)) <= 1e-3
+    assert np.max(np.abs(lift32 - lift64)) <= 1e-3 * max(np.abs(lift64).max(), 1e-12)
