@@ -66,9 +66,10 @@ def workload(name: str, size: int = 4096) -> dict:
                     inlet=("parabolic", 0.05, 1, 254), outlet_bc=2, rho_out=1.0, ref_args=[
                         "--collision", "trt", "--tau-even", repr(te), "--magic", "0.25", "--inlet", "zh",
                         "--outlet", "zhp", "--inlet-u", "parabolic:0.05:1:254", "--outlet-u", "pressure"])
-    if name == "cavity129":
-        return dict(name=name, desc="lid-driven cavity 129x129, BGK tau 0.884, lid u=(0.1,0)",
-                    types=lambda: W.cavity_types(129), collision=0, tau=0.884, tau_even=0.884, tau_odd=0.884,
+    if name in ("cavity129", "cavity"):
+        n = 129 if name == "cavity129" else size
+        return dict(name=f"cavity{n}", desc=f"lid-driven cavity {n}x{n}, BGK tau 0.884, lid u=(0.1,0)",
+                    types=lambda: W.cavity_types(n), collision=0, tau=0.884, tau_even=0.884, tau_odd=0.884,
                     inlet=("const", 0.1, 0.0), outlet_bc=0, rho_out=1.0, ref_args=[
                         "--collision", "bgk", "--tau", "0.884", "--inlet", "zh", "--outlet", "zh",
                         "--inlet-u", "const:0.1:0"])
@@ -278,8 +279,12 @@ def make_lattice(L, wl, nodes, R, C, storage, device):
     return g
 
 
-def time_form(L, wl, nodes, R, C, storage, device, warmup, steps, dist, sampler=None):
+def time_form(L, wl, nodes, R, C, storage, device, warmup, steps, dist, pipeline=None, launch_shape=None):
     g = make_lattice(L, wl, nodes, R, C, storage, device)
+    if pipeline is not None:
+        g.set_pipeline(pipeline)
+    if launch_shape is not None:
+        g.set_launch_shape(launch_shape)
     g.init()
     g.step(warmup)
     g.synchronize()
@@ -344,7 +349,8 @@ def run_ours(a, dist):
     for storage, name, sb in ((0, "f64", 8), (1, "f32s", 4), (2, "f16s", 2)):
         if name not in a.forms.split(","):
             continue
-        g, ms, (t0, t1), u = time_form(L, wl, nodes, R, C, storage, dev, a.warmup, a.steps, dist)
+        g, ms, (t0, t1), u = time_form(L, wl, nodes, R, C, storage, dev, a.warmup, a.steps, dist, a.pipeline,
+                                       a.launch_shape)
         per = ms / a.steps
         bps = bytes_per_step(sb, n_active, R * C)
         form = {"mlups": dist.world * R * C / per / 1e3, "ms_per_step": per, "gb_s": bps / per / 1e6,
@@ -503,7 +509,7 @@ def run_batch(a, dist):
         "roofline": {"bound": "hbm", "achieved": round(bps / per / 1e6, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(bps / per / 1e6 / peak, 4), "traffic": None},
         "plain_f64": {"mlups": round(plain, 1), "steps_per_problem": k_plain,
-                      "path": "each problem alone through llb_step (FP64, TMA pipeline)"},
+                      "path": "each problem alone through llb_step (FP64, the lattice's default step kernel)"},
         "batched_over_plain_f64": round(batched / plain, 3),
         "gpu_launches": (a.steps + spl - 1) // spl, "clocks": sampler.summary(t0, t1),
     }
@@ -669,9 +675,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="porous4096",
-                    choices=("porous4096", "cylinder1024x256", "cavity129", "batch256", "serve"))
+                    choices=("porous4096", "cylinder1024x256", "cavity129", "cavity", "batch256", "serve"))
+    ap.add_argument("--pipeline", type=int, default=None,
+                    help="plain path step kernel: -1 one thread per node, 0..2 TMA configurations (default: per lattice)")
+    ap.add_argument("--launch-shape", type=int, default=None, help="columns per block of the one-thread kernel")
     ap.add_argument("--requests", type=int, default=96, help="requests in the served stream (workload serve)")
-    ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous workload")
+    ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous and cavity workloads")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
