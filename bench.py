@@ -149,18 +149,24 @@ class ClockSampler:
 # distributed plumbing (replicas)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self, gpus: int):
+    """One process per GPU (torchrun environment); replicas, timing = max over
+    ranks.  backend "gloo" runs the same logic on CPU tensors."""
+
+    def __init__(self, gpus: int, backend: str = "nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import torch
             import torch.distributed as dist
             from datetime import timedelta
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = f"cuda:{self.local}"
+            dist.init_process_group(backend, timeout=timedelta(seconds=300))
             self.pg = dist
             self.torch = torch
 
@@ -171,7 +177,7 @@ class Dist:
     def max(self, x: float) -> float:
         if not self.pg:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 

@@ -181,3 +181,27 @@ def test_large_lattices_step_by_their_own_kernel_in_the_batch():
         check_against_oracle(b.lattice(a), big_por, 111)
         check_against_oracle(b.lattice(s), PROBLEMS[1], 111)
         check_against_oracle(b.lattice(c), big_cav, 71)
+
+
+def test_batch_f16s_matches_single_lattice():
+    import llalbm_cuda as L
+
+    steps = 300
+    singles = []
+    for name, lists, p, ins, outs in PROBLEMS:
+        tab = gpu_table(lists, p, ins, outs, steps + 2)
+        with L.CudaLattice(lists.rows, lists.cols, lists.fluid, lists.wall, lists.inlet, lists.inlet_side,
+                           lists.outlet, lists.outlet_side, lists.obstacle, lists.obstacle_dirs, collision=p.collision,
+                           tau=p.tau, tau_even=p.tau_even, tau_odd=p.tau_odd, inlet_bc=p.inlet_bc,
+                           outlet_bc=p.outlet_bc, storage=L.STORE_F16S, open_table_rows=tab.shape[0]) as g:
+            g.set_open_values(tab)
+            g.init()
+            g.step(steps - 1)
+            singles.append(g.compute_macro()[1])
+    with L.CudaBatch(storage=L.STORE_F16S) as b:
+        slots = [add(b, prob, steps + 2) for prob in PROBLEMS]
+        b.step(steps - 1)
+        for slot, u1, prob in zip(slots, singles, PROBLEMS):
+            u = b.lattice(slot).compute_macro()[1]
+            err = np.sqrt(((u - u1) ** 2).sum() / max((u1 ** 2).sum(), 1e-30))
+            assert err <= 1e-6, (prob[0], err)
