@@ -87,21 +87,19 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     if (inside && class_active(cls)) {
         typename M::R f[9];
         pull<M>(g, fin, i, j, node, m, warp_plain, f);
-        double rho, ux, uy;
-        typename M::R rr;
+        typename M::R rr, xr, yr;
         if (cls == CLS_OPEN) {
+            double rho, ux, uy;
             open_node<M>(Lp->ot, g.open_idx[node], m, t, f, rho, ux, uy);
             rr = M::from_f64(rho);
+            xr = static_cast<typename M::R>(ux);
+            yr = static_cast<typename M::R>(uy);
         } else {
-            typename M::R r, x, y;
-            M::moments(f, r, x, y);
-            rr = r;
-            ux = x;
-            uy = y;
-            bad = !isfinite(M::rho_f64(r));
+            M::moments(f, rr, xr, yr);
+            bad = !M::finite(rr);
         }
-        if (Lp->c.model == 0) M::template collide<0>(f, rr, ux, uy, Lp->c);
-        else M::template collide<1>(f, rr, ux, uy, Lp->c);
+        if (Lp->c.model == 0) M::template collide<0>(f, rr, xr, yr, Lp->c);
+        else M::template collide<1>(f, rr, xr, yr, Lp->c);
 #pragma unroll
         for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
     } else if (write_sector && j < g.cols && i < g.ld) {

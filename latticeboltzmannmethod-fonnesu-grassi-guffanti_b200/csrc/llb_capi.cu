@@ -432,6 +432,11 @@ int llb_create(const llb_desc* d, llb_handle* out) {
         h->coll.he = 0.5 * (1.0 / d->tau_even);
         h->coll.ho = 0.5 * (1.0 / d->tau_odd);
     }
+    h->coll.tf = static_cast<float>(h->coll.t);
+    h->coll.omtf = static_cast<float>(h->coll.omt);
+    h->coll.ief = static_cast<float>(h->coll.ie);
+    h->coll.hef = static_cast<float>(h->coll.he);
+    h->coll.hof = static_cast<float>(h->coll.ho);
 
     std::vector<uint8_t> mask, bb;
     std::vector<int32_t> open_idx;

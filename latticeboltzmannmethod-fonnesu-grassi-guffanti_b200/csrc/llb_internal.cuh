@@ -93,6 +93,8 @@ struct Collision {
     double t, omt;
     // TRT: ie = 1/tau_even, he = 0.5*(1/tau_even), ho = 0.5*(1/tau_odd)   (TRTCollision.hpp:155-188)
     double ie, he, ho;
+    // the same rates rounded to FP32 for the shifted storage forms
+    float tf, omtf, ief, hef, hof;
 };
 
 struct MacroOut {

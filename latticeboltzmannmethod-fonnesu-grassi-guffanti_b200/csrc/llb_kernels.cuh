@@ -138,29 +138,27 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
             } else {
                 pull<M>(g, fin, i, j, node, m, warp_plain, f);
             }
-            double rho, ux, uy;
-            typename M::R rr;
+            // moments stay in the model's arithmetic type up to the collision
+            typename M::R rr, xr, yr;
             if (cls == CLS_OPEN) {
                 const long long t = INIT ? 0 : current_step(ss);
+                double rho, ux, uy;
                 open_node<M>(ot, g.open_idx[node], m, t, f, rho, ux, uy);
                 rr = M::from_f64(rho);
+                xr = static_cast<typename M::R>(ux);
+                yr = static_cast<typename M::R>(uy);
             } else {
-                typename M::R r, x, y;
-                M::moments(f, r, x, y);
-                rr = r;
-                ux = x;
-                uy = y;
-                rho = M::rho_f64(r);
-                bad = !isfinite(rho);
+                M::moments(f, rr, xr, yr);
+                bad = !M::finite(rr);
             }
             if (MACRO) {
                 const long long d = static_cast<long long>(j) * g.rows + i;
                 const long long N = static_cast<long long>(g.rows) * g.cols;
-                mo.rho[d] = rho;
-                mo.u[d] = ux;
-                mo.u[d + N] = uy;
+                mo.rho[d] = M::rho_f64(rr);
+                mo.u[d] = xr;
+                mo.u[d + N] = yr;
             }
-            M::template collide<COLL>(f, rr, ux, uy, c);
+            M::template collide<COLL>(f, rr, xr, yr, c);
 #pragma unroll
             for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
         } else {

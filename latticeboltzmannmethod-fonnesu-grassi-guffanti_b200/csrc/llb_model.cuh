@@ -168,6 +168,7 @@ struct ModelF64 {
     }
 
     static __device__ __forceinline__ double rho_f64(R rho) { return rho; }
+    static __device__ __forceinline__ bool finite(R rho) { return isfinite(rho); }
     static __device__ __forceinline__ R from_f64(double v) { return v; }
 };
 
@@ -265,38 +266,51 @@ struct ModelShift {
     }
 
     // shifted equilibrium g_eq = w_k * (drho + rho*(3cu + 4.5cu^2 - 1.5u^2)), then
-    // BGK or TRT on the shifted values (the shifts cancel in both operators)
+    // BGK or TRT on the shifted values (the shifts cancel in both operators).
+    // Opposite directions k, opp(k) share w_k and cu^2 and differ in the sign
+    // of cu, so each pair is computed once: g_eq = w (even +- odd).
     template <int COLL>
-    static __device__ __forceinline__ void collide(R* g, double drho_d, double ux_d, double uy_d, const Collision& c) {
-        const R drho = static_cast<R>(drho_d), ux = static_cast<R>(ux_d), uy = static_cast<R>(uy_d);
+    static __device__ __forceinline__ void collide(R* g, R drho, R ux, R uy, const Collision& c) {
         const R rho = 1.0f + drho;
         const R u2 = 1.5f * (ux * ux + uy * uy);
-        R e[9];
-        e[0] = w_f32(0) * (drho - rho * u2);
+        const R e0 = w_f32(0) * (drho - rho * u2);
+        // pairs (1,3), (2,4), (5,7), (6,8): cu of the first direction of each pair
+        constexpr int first[4] = {1, 2, 5, 6};
+        R ev[4], od[4];
 #pragma unroll
-        for (int k = 1; k < 9; ++k) {
+        for (int p = 0; p < 4; ++p) {
+            const int k = first[p];
             const R cu = static_cast<R>(DJ(k)) * ux - static_cast<R>(DI(k)) * uy;
-            e[k] = w_f32(k) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - u2));
+            ev[p] = w_f32(k) * (drho + rho * (4.5f * cu * cu - u2));
+            od[p] = w_f32(k) * (rho * (3.0f * cu));
         }
         if (COLL == 0) {
-            const R t = static_cast<R>(c.t), omt = static_cast<R>(c.omt);
+            const R t = c.tf, omt = c.omtf;
+            g[0] = omt * g[0] + t * e0;
 #pragma unroll
-            for (int k = 0; k < 9; ++k) g[k] = omt * g[k] + t * e[k];
+            for (int p = 0; p < 4; ++p) {
+                const int k = first[p], b = opp(k);
+                g[k] = omt * g[k] + t * (ev[p] + od[p]);
+                g[b] = omt * g[b] + t * (ev[p] - od[p]);
+            }
         } else {
-            const R ie = static_cast<R>(c.ie), he = static_cast<R>(c.he), ho = static_cast<R>(c.ho);
-            R q[9];
+            const R ie = c.ief, he = c.hef, ho = c.hof;
+            g[0] = g[0] - ie * (g[0] - e0);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) q[k] = g[k];
-            g[0] = q[0] - ie * (q[0] - e[0]);
-#pragma unroll
-            for (int k = 1; k < 9; ++k) {
-                const int b = opp(k);
-                g[k] = q[k] - he * ((q[k] + q[b]) - (e[k] + e[b])) - ho * ((q[k] - q[b]) - (e[k] - e[b]));
+            for (int p = 0; p < 4; ++p) {
+                const int k = first[p], b = opp(k);
+                // symmetric and antisymmetric non-equilibrium parts of the pair
+                const R sym = (g[k] + g[b]) - 2.0f * ev[p];
+                const R asym = (g[k] - g[b]) - 2.0f * od[p];
+                const R qk = g[k], qb = g[b];
+                g[k] = qk - he * sym - ho * asym;
+                g[b] = qb - he * sym + ho * asym;
             }
         }
     }
 
     static __device__ __forceinline__ double rho_f64(R drho) { return 1.0 + static_cast<double>(drho); }
+    static __device__ __forceinline__ bool finite(R drho) { return isfinite(drho); }
     static __device__ __forceinline__ R from_f64(double v) { return static_cast<R>(v - 1.0); }
 };
 

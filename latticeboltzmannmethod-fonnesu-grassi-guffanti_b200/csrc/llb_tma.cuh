@@ -203,8 +203,7 @@ __global__ void __launch_bounds__(CFG::THREADS, 1)
                         f[k] = M::load(p);
                     }
                 }
-                double rho, ux, uy;
-                R rr;
+                R rr, xr, yr;
                 if (cls == CLS_OPEN) {
                     // sources outside the lattice (the boxes read zeros there) keep w_k
 #pragma unroll
@@ -212,17 +211,16 @@ __global__ void __launch_bounds__(CFG::THREADS, 1)
                         const int si = i - DI(k), sj = j - DJ(k);
                         if (si < 0 || sj < 0 || si >= g.rows || sj >= g.cols) f[k] = M::keep(k);
                     }
+                    double rho, ux, uy;
                     open_node<M>(ot, g.open_idx[node], m, current_step(ss), f, rho, ux, uy);
                     rr = M::from_f64(rho);
+                    xr = static_cast<R>(ux);
+                    yr = static_cast<R>(uy);
                 } else {
-                    R r, x, y;
-                    M::moments(f, r, x, y);
-                    rr = r;
-                    ux = x;
-                    uy = y;
-                    bad |= !isfinite(M::rho_f64(r));
+                    M::moments(f, rr, xr, yr);
+                    bad |= !M::finite(rr);
                 }
-                M::template collide<COLL>(f, rr, ux, uy, c);
+                M::template collide<COLL>(f, rr, xr, yr, c);
 #pragma unroll
                 for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
             } else if (write_sector && j < g.cols && i < g.ld) {
