@@ -215,6 +215,15 @@ int llb_batch_destroy(llb_batch_handle b);
 int llb_batch_add(llb_batch_handle b, const llb_desc* desc, const double* open_values, int32_t rows,
                   int32_t* slot);
 int llb_batch_remove(llb_batch_handle b, int32_t slot);
+/* Moves a lattice made by llb_create (boundary values set; initialised or
+   not -- step 0 then runs on the batch's stream) into the batch, so its
+   creation and upload can happen elsewhere (another thread, another stream)
+   while the batch runs.  The batch owns it from then on. */
+int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot);
+/* Takes a lattice out of the batch without destroying it: the caller owns
+   the handle again (on a stream of its own that starts after the batch work
+   queued so far) and destroys it with llb_destroy. */
+int llb_batch_detach(llb_batch_handle b, int32_t slot, llb_handle* out);
 /* Advances every lattice of the batch by nsteps. */
 int llb_batch_step(llb_batch_handle b, int32_t nsteps);
 int llb_batch_lattice(llb_batch_handle b, int32_t slot, llb_handle* out);
@@ -230,6 +239,11 @@ int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, in
 int llb_batch_get_step(llb_batch_handle b, int64_t* step);
 /* Waits for the batch; LLB_E_TIMEOUT if a cooperative launch gave up a grid barrier. */
 int llb_batch_synchronize(llb_batch_handle b);
+/* Scheduling priority of the batch's stream (CUDA stream priorities: a lower
+   number is a higher priority; clamped to the device's range, so INT32_MIN
+   asks for the highest).  Blocks of a higher-priority stream are scheduled
+   before waiting blocks of lower-priority streams.  Only on an empty batch. */
+int llb_batch_set_stream_priority(llb_batch_handle b, int32_t priority);
 int llb_batch_event_record(llb_batch_handle b, int32_t slot);
 int llb_batch_event_elapsed_ms(llb_batch_handle b, int32_t slot_begin, int32_t slot_end, float* ms);
 int llb_batch_info(llb_batch_handle b, int64_t* lattices, int64_t* nodes, int64_t* device_bytes);
@@ -239,12 +253,15 @@ const char* llb_batch_last_error(llb_batch_handle b);
 /* A request loop over a batch; no counterpart in the reference (one Lattice
    per process, driven by its own main()).  Requests -- a lattice description,
    its boundary values for steps 0..rows-1 and a step count -- are submitted
-   from any thread and queued; one worker thread admits them first come, first
-   served while the device bytes of the admitted lattices fit budget_bytes,
-   keeps their state resident and advances them (batched mode: together, one
-   batch, in chunks of at most max_chunk_steps, admitting arrivals between
-   chunks while the previous chunk runs; sequential mode: one at a time
-   through the plain single-lattice path).  A request of `steps` steps (>= 2)
+   from any thread and queued; they are admitted first come, first served
+   while the device bytes of the admitted lattices fit budget_bytes, and their
+   state stays resident until they finish.  Batched mode: a preparer thread
+   creates admitted lattices while the GPU runs, a worker advances them in two
+   concurrent lanes (lattices under 2^20 nodes in one work-list batch on a
+   high-priority stream, larger ones by their own launches), in chunks of at
+   most max_chunk_steps for the large lane, and a reaper thread copies results
+   and frees.  Sequential mode: one request at a time through the plain
+   single-lattice path.  A request of `steps` steps (>= 2)
    ends with the state the reference's Lattice holds after perform_lbm(steps)
    and returns that call's rho and u: steps - 1 collisions and the macroscopic
    fields of the last step (llb_compute_macro).  The lattice's storage, device
@@ -258,11 +275,14 @@ const char* llb_batch_last_error(llb_batch_handle b);
 #define LLB_REQ_FAILED 3
 typedef struct llb_server* llb_server_handle;
 /* completed / failed requests, lattice-node updates of the completed ones,
-   requests queued and running now, device bytes charged, chunks launched and
-   the batch steps they ran (one persistent launch each), the clock now. */
+   requests queued and admitted-but-unfinished now, device bytes charged,
+   chunks launched and the lane steps they ran, the clock now, and the
+   seconds the batched mode's threads spent creating lattices (preparer),
+   waiting for chunks (worker) and copying results and freeing (reaper). */
 typedef struct {
     int64_t completed, failed, node_steps, queued, running, bytes_in_use, chunks, batch_steps;
     double clock_s;
+    double admit_s, wait_s, retire_s;
 } llb_server_counters;
 int llb_server_create(int32_t device, int32_t storage, int32_t mode, int64_t budget_bytes, int32_t max_chunk_steps,
                       llb_server_handle* out);

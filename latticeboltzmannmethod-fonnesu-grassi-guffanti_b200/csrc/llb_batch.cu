@@ -299,18 +299,33 @@ int llb_batch_add(llb_batch_handle b, const llb_desc* desc, const double* open_v
     llb_handle h = nullptr;
     int rc = llb_create(desc, &h);
     if (rc != LLB_OK) return bfail(b, rc, llb_last_error(nullptr));
-    // the lattice works on the batch's stream from now on
-    cudaStreamSynchronize(h->stream);
-    cudaStreamDestroy(h->stream);
-    h->stream = b->stream;
-    h->own_stream = false;
     if (open_values && rows > 0 && (rc = llb_set_open_values(h, 0, rows, open_values)) != LLB_OK) {
         llb_destroy(h);
         return bfail(b, rc, "boundary values rejected");
     }
-    if ((rc = llb_init(h, 0)) != LLB_OK) {
-        llb_destroy(h);
-        return bfail(b, rc, "llb_init failed");
+    if ((rc = llb_batch_attach(b, h, slot)) != LLB_OK) llb_destroy(h);
+    return rc;
+}
+
+int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
+    if (!b || !h || !slot) return LLB_E_INVALID;
+    if (h->storage != b->storage || h->pattern != LLB_PATTERN_AB || h->device != b->device)
+        return bfail(b, LLB_E_INVALID, "lattice storage, pattern or device differs from the batch");
+    if (!h->own_stream) return bfail(b, LLB_E_STATE, "lattice already belongs to a batch");
+    if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    // the lattice works on the batch's stream from now on
+    LLB_BCUDA(b, cudaStreamSynchronize(h->stream));
+    cudaStreamDestroy(h->stream);
+    h->stream = b->stream;
+    h->own_stream = false;
+    if (!h->initialized) {
+        const int rc = llb_init(h, 0);
+        if (rc != LLB_OK) {
+            // give the handle a stream of its own again so the caller can destroy it
+            cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+            h->own_stream = true;
+            return bfail(b, rc, "llb_init failed");
+        }
     }
     BatchLattice d{};
     const LaunchCtx x = handle_ctx(h);
@@ -334,6 +349,31 @@ int llb_batch_add(llb_batch_handle b, const llb_desc* desc, const double* open_v
     b->desc[s] = d;
     b->dirty = true;
     *slot = s;
+    return LLB_OK;
+}
+
+int llb_batch_detach(llb_batch_handle b, int32_t slot, llb_handle* out) {
+    if (!b || !out || slot < 0 || slot >= static_cast<int>(b->slot.size()) || !b->slot[slot]) return LLB_E_INVALID;
+    if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    sync_handle(b, slot);
+    llb_handle h = b->slot[slot];
+    // the handle's own stream starts after the batch work queued so far
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    LLB_BCUDA(b, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, b->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev, 0);
+    if (ev) cudaEventDestroy(ev);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(st);
+        return bfail(b, LLB_E_CUDA, std::string("detach: ") + cudaGetErrorString(e));
+    }
+    h->stream = st;
+    h->own_stream = true;
+    b->slot[slot] = nullptr;
+    b->dirty = true;
+    *out = h;
     return LLB_OK;
 }
 
@@ -436,6 +476,23 @@ int llb_batch_synchronize(llb_batch_handle b) {
         cudaMemset(b->d_err, 0, sizeof(unsigned));
         return bfail(b, LLB_E_TIMEOUT, "batched kernel gave up a grid barrier");
     }
+    return LLB_OK;
+}
+
+int llb_batch_set_stream_priority(llb_batch_handle b, int32_t priority) {
+    if (!b) return LLB_E_INVALID;
+    for (llb_handle h : b->slot)
+        if (h) return bfail(b, LLB_E_STATE, "stream priority can only change on an empty batch");
+    cudaSetDevice(b->device);
+    int lo = 0, hi = 0;
+    LLB_BCUDA(b, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    const int p = std::min(std::max(static_cast<int>(priority), hi), lo);  // hi is the greatest priority
+    cudaStream_t st = nullptr;
+    LLB_BCUDA(b, cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, p));
+    LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+    drop_graph(b);
+    cudaStreamDestroy(b->stream);
+    b->stream = st;
     return LLB_OK;
 }
 

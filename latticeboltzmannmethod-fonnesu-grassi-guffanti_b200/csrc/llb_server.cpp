@@ -1,16 +1,25 @@
 // Solve server (C ABI llb_server_*).  Requests -- one lattice, its boundary
-// values and a step count -- arrive from any thread.  One worker thread keeps
-// every admitted lattice resident on the device and advances them together.
+// values and a step count -- arrive from any thread and are served by native
+// threads that keep every admitted lattice resident on the device.
 //
-// Batched mode (continuous batching): requests are admitted first come, first
-// served while their device memory fits the budget.  The worker advances the
-// running batch in chunks of at most max_chunk steps, never past the earliest
-// completion.  Admission of newly arrived requests (mask build, allocation,
-// upload, step 0) happens on the host while the previous chunk is still running
-// on the device, and they join the batch at the next chunk boundary, so their
-// work overlaps the work of the requests already running.  A finished request's
-// result -- rho and u of the state after its last step -- is copied to host
-// memory and its lattice is freed, which makes room for the queue.
+// Batched mode (continuous batching) runs three threads:
+//  * preparer threads admit queued requests first come, first served while
+//    their device memory fits the budget, and create each lattice (mask build,
+//    allocation, upload) on a stream of its own, several at a time;
+//  * the worker moves prepared lattices into one of two lanes, each a batch on
+//    its own stream -- lattices of fewer than 2^20 nodes share the work-list
+//    kernel (small lane), larger ones are stepped by their own launches (large
+//    lane) -- and advances the lanes chunk by chunk.  The lanes run
+//    concurrently; the small lane's stream has the higher scheduling priority,
+//    so a small request keeps its own step rate beside large lattices.  Each
+//    chunk the large lane runs at most max_chunk steps and the small lane as
+//    many steps as fit in the same time (measured per-step times), each never
+//    past its earliest completion; prepared lattices join at the next chunk
+//    boundary, so their work overlaps the work already running;
+//  * the reaper takes finished lattices out of the worker's way, copies their
+//    result -- the rho and u the reference's Lattice holds after
+//    perform_lbm(steps) -- to host memory and frees them, which returns their
+//    bytes to the budget.
 //
 // Sequential mode serves the same requests one at a time through the plain
 // single-lattice path (the comparison for the batched mode).
@@ -19,6 +28,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -52,6 +62,8 @@ struct Request {
     int state = LLB_REQ_QUEUED;
     int64_t bytes = 0;          // device bytes charged against the budget
     double t_submit = 0, t_admit = 0, t_done = 0;
+    llb_handle h = nullptr;     // the lattice while it is prepared, running or retired
+    int rc = LLB_OK;            // outcome of its steps
     std::vector<double> rho, u;
     std::string error;
 };
@@ -76,38 +88,38 @@ struct llb_server {
     int mode = LLB_SERVE_BATCHED;
     int64_t budget = 0;
     int32_t max_chunk = 256;
-    llb_batch_handle batch = nullptr;
+    llb_batch_handle batch[2] = {nullptr, nullptr};  // small lane, large lane
     std::mutex mu;
-    std::condition_variable cv_work;   // the worker: new requests or stop
+    std::condition_variable cv_prep;   // the preparer: queued requests, freed bytes, stop
+    std::condition_variable cv_work;   // the worker: prepared lattices, stop
+    std::condition_variable cv_reap;   // the reaper: finished lattices, worker done
     std::condition_variable cv_done;   // waiters: a request finished
-    std::deque<std::shared_ptr<Request>> queue;
+    std::deque<std::shared_ptr<Request>> queue;   // submitted, not admitted
+    std::deque<std::shared_ptr<Request>> ready;   // created on the device, waiting for a lane
+    std::deque<std::shared_ptr<Request>> dying;   // out of their lane, waiting for the result copy
     std::map<int64_t, std::shared_ptr<Request>> all;
-    std::vector<std::shared_ptr<Request>> running;   // touched by the worker only
-    int64_t n_running = 0;
+    std::vector<std::shared_ptr<Request>> running[2];  // per lane; touched by the worker only
+    int64_t admitted = 0;              // admitted and not finished
     int64_t next_id = 1;
     int64_t in_use = 0;
-    bool stop = false;
-    std::thread worker;
+    bool stop = false, preparer_done = false, worker_done = false;
+    int preparers_live = 0;
+    std::vector<std::thread> preparers;
+    std::thread worker, reaper;
     int64_t node_steps = 0;
     int64_t completed = 0;
     int64_t failed = 0;
     int64_t chunks = 0;
     int64_t batch_steps = 0;
+    double admit_s = 0, wait_s = 0, retire_s = 0;
     std::string error;
 };
 
 namespace {
 
-// Marks a request finished (rc == LLB_OK: reads its result through h first).
-void finish(llb_server_handle s, const std::shared_ptr<Request>& r, llb_handle h, int rc, const char* what) {
-    if (rc == LLB_OK) {
-        const size_t N = static_cast<size_t>(r->desc.rows * r->desc.cols);
-        r->rho.resize(N);
-        r->u.resize(2 * N);
-        rc = llb_compute_macro(h, r->rho.data(), r->u.data());
-    }
-    std::string msg;
-    if (rc != LLB_OK) msg = std::string(what) + ": " + (h ? llb_last_error(h) : llb_last_error(nullptr));
+// Marks a request finished and returns its bytes to the budget (its lattice
+// is already destroyed).
+void complete(llb_server_handle s, const std::shared_ptr<Request>& r, int rc, const std::string& msg) {
     std::lock_guard<std::mutex> lk(s->mu);
     r->t_done = now_s();
     if (rc == LLB_OK) {
@@ -122,26 +134,42 @@ void finish(llb_server_handle s, const std::shared_ptr<Request>& r, llb_handle h
         s->failed += 1;
     }
     s->in_use -= r->bytes;
+    s->admitted -= 1;
     s->cv_done.notify_all();
+    s->cv_prep.notify_all();
+}
+
+// Copies the result of a finished lattice (rc == LLB_OK) and destroys it.
+void retire(llb_server_handle s, const std::shared_ptr<Request>& r, int rc, const char* what) {
+    llb_handle h = r->h;
+    if (rc == LLB_OK) {
+        const size_t N = static_cast<size_t>(r->desc.rows * r->desc.cols);
+        r->rho.resize(N);
+        r->u.resize(2 * N);
+        rc = llb_compute_macro(h, r->rho.data(), r->u.data());
+    }
+    std::string msg;
+    if (rc != LLB_OK) msg = std::string(what) + ": " + (h ? llb_last_error(h) : llb_last_error(nullptr));
+    if (h) llb_destroy(h);
+    r->h = nullptr;
+    complete(s, r, rc, msg);
 }
 
 // One request through the plain single-lattice path: steps - 1 collisions
 // (llb_init is the first), then rho and u of the state the last step reads.
 void serve_plain(llb_server_handle s, const std::shared_ptr<Request>& r) {
-    llb_handle h = nullptr;
     llb_desc d = r->desc;
-    int rc = llb_create(&d, &h);
-    if (rc == LLB_OK && r->rows > 0) rc = llb_set_open_values(h, 0, r->rows, r->values.data());
-    if (rc == LLB_OK) rc = llb_init(h, 0);
+    int rc = llb_create(&d, &r->h);
+    if (rc == LLB_OK && r->rows > 0) rc = llb_set_open_values(r->h, 0, r->rows, r->values.data());
+    if (rc == LLB_OK) rc = llb_init(r->h, 0);
     int64_t left = r->steps - 2;
     while (rc == LLB_OK && left > 0) {
         const int32_t n = static_cast<int32_t>(std::min<int64_t>(left, 1 << 20));
-        rc = llb_step(h, n, 0);
+        rc = llb_step(r->h, n, 0);
         left -= n;
     }
-    if (rc == LLB_OK) rc = llb_synchronize(h);
-    finish(s, r, h, rc, "plain path");
-    if (h) llb_destroy(h);
+    if (rc == LLB_OK) rc = llb_synchronize(r->h);
+    retire(s, r, rc, "plain path");
 }
 
 void sequential_loop(llb_server_handle s) {
@@ -149,113 +177,188 @@ void sequential_loop(llb_server_handle s) {
         std::shared_ptr<Request> r;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+            s->cv_prep.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             if (s->queue.empty()) return;  // stop requested and nothing left
             r = s->queue.front();
             s->queue.pop_front();
             r->state = LLB_REQ_RUNNING;
             r->t_admit = now_s();
             s->in_use += r->bytes;
-            s->n_running = 1;
+            s->admitted += 1;
         }
         serve_plain(s, r);
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->n_running = 0;
     }
 }
 
-// Admits queued requests while the budget allows (the queue head always when
-// nothing runs); returns them in arrival order.
-std::vector<std::shared_ptr<Request>> take_admissible(llb_server_handle s, bool block) {
-    std::vector<std::shared_ptr<Request>> out;
-    std::unique_lock<std::mutex> lk(s->mu);
-    if (block) s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-    while (!s->queue.empty()) {
-        auto& r = s->queue.front();
-        if (s->in_use + r->bytes > s->budget && !(s->running.empty() && out.empty())) break;
-        r->state = LLB_REQ_RUNNING;
-        r->t_admit = now_s();
-        s->in_use += r->bytes;
-        out.push_back(r);
-        s->queue.pop_front();
+constexpr int64_t LARGE_LANE_NODES = 1 << 20;
+
+int lane_of(const Request& r) { return r.desc.rows * r.desc.cols >= LARGE_LANE_NODES ? 1 : 0; }
+
+void preparer_loop(llb_server_handle s) {
+    for (;;) {
+        std::shared_ptr<Request> r;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_prep.wait(lk, [&] {
+                return s->stop ||
+                       (!s->queue.empty() && (s->in_use + s->queue.front()->bytes <= s->budget || s->admitted == 0));
+            });
+            if (s->stop) {
+                if (--s->preparers_live == 0) {
+                    s->preparer_done = true;
+                    s->cv_work.notify_all();
+                }
+                return;
+            }
+            r = s->queue.front();
+            s->queue.pop_front();
+            r->state = LLB_REQ_RUNNING;
+            r->t_admit = now_s();
+            s->in_use += r->bytes;
+            s->admitted += 1;
+        }
+        const double t0 = now_s();
+        llb_desc d = r->desc;
+        int rc = llb_create(&d, &r->h);
+        if (rc == LLB_OK && r->rows > 0) rc = llb_set_open_values(r->h, 0, r->rows, r->values.data());
+        if (rc == LLB_OK) rc = llb_synchronize(r->h);
+        int64_t actual = 0;
+        if (rc == LLB_OK) rc = llb_device_bytes(r->h, &actual);
+        if (rc != LLB_OK) {
+            retire(s, r, rc, "admission failed");
+            continue;
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->in_use += actual - r->bytes;
+        r->bytes = actual;
+        s->admit_s += now_s() - t0;
+        s->ready.push_back(r);
+        s->cv_work.notify_all();
     }
-    return out;
+}
+
+void reaper_loop(llb_server_handle s) {
+    for (;;) {
+        std::shared_ptr<Request> r;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_reap.wait(lk, [&] { return !s->dying.empty() || s->worker_done; });
+            if (s->dying.empty()) return;
+            r = s->dying.front();
+            s->dying.pop_front();
+        }
+        const double t0 = now_s();
+        retire(s, r, r->rc, "batched step");
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->retire_s += now_s() - t0;
+    }
 }
 
 void batched_loop(llb_server_handle s) {
-    bool inflight = false;   // a chunk was launched and not yet waited for
+    bool inflight[2] = {false, false};  // a chunk was launched on the lane and not yet waited for
+    int64_t launched[2] = {0, 0};       // steps of that chunk
+    double ms_step[2] = {0.0, 0.0};     // measured device time per step (0: not measured yet)
     for (;;) {
-        const bool idle = s->running.empty() && !inflight;
+        const bool idle = s->running[0].empty() && s->running[1].empty() && !inflight[0] && !inflight[1];
+        std::deque<std::shared_ptr<Request>> joining;
         {
-            std::lock_guard<std::mutex> lk(s->mu);
-            if (idle && s->stop && s->queue.empty()) return;
-        }
-        // 1. admissions (overlap the chunk in flight)
-        for (auto& r : take_admissible(s, idle)) {
-            llb_desc d = r->desc;
-            int32_t slot = -1;
-            const int rc = llb_batch_add(s->batch, &d, r->rows > 0 ? r->values.data() : nullptr, r->rows, &slot);
-            if (rc != LLB_OK) {
-                std::lock_guard<std::mutex> lk(s->mu);
-                r->state = LLB_REQ_FAILED;
-                r->error = std::string("admission failed: ") + llb_batch_last_error(s->batch);
-                r->t_done = now_s();
-                s->in_use -= r->bytes;
-                s->failed += 1;
-                s->cv_done.notify_all();
-                continue;
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (idle) s->cv_work.wait(lk, [&] { return !s->ready.empty() || s->preparer_done; });
+            if (idle && s->ready.empty() && s->preparer_done) {
+                s->worker_done = true;
+                s->cv_reap.notify_all();
+                return;
             }
-            llb_handle h = nullptr;
-            int64_t actual = 0;
-            if (llb_batch_lattice(s->batch, slot, &h) == LLB_OK && llb_device_bytes(h, &actual) == LLB_OK) {
+            joining.swap(s->ready);
+        }
+        // 1. prepared lattices join their lane (step 0 queued on the lane's stream)
+        for (auto& r : joining) {
+            const int ln = lane_of(*r);
+            int32_t slot = -1;
+            const int rc = llb_batch_attach(s->batch[ln], r->h, &slot);
+            if (rc != LLB_OK) {
+                r->rc = rc;
                 std::lock_guard<std::mutex> lk(s->mu);
-                s->in_use += actual - r->bytes;
-                r->bytes = actual;
+                s->dying.push_back(r);
+                s->cv_reap.notify_all();
+                continue;
             }
             r->slot = slot;
-            r->remaining = r->steps - 2;  // llb_batch_add ran the first collision
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->running.push_back(r);
-            s->n_running = static_cast<int64_t>(s->running.size());
+            r->remaining = r->steps - 2;  // step 0 was the first collision
+            s->running[ln].push_back(r);
         }
-        // 2. wait for the chunk in flight, retire what it finished
-        int rc = LLB_OK;
-        if (inflight) {
-            rc = llb_batch_synchronize(s->batch);
-            inflight = false;
-        }
-        std::vector<std::shared_ptr<Request>> keep;
-        for (auto& r : s->running) {
-            if (r->remaining > 0 && rc == LLB_OK) {
-                keep.push_back(r);
-                continue;
+        // 2. per lane: wait for the chunk in flight, hand what it finished to the reaper
+        for (int ln = 0; ln < 2; ++ln) {
+            llb_batch_handle b = s->batch[ln];
+            int rc = LLB_OK;
+            if (inflight[ln]) {
+                const double t0 = now_s();
+                rc = llb_batch_synchronize(b);
+                float ms = 0.f;
+                if (rc == LLB_OK && launched[ln] > 0 && llb_batch_event_elapsed_ms(b, 0, 1, &ms) == LLB_OK)
+                    ms_step[ln] = static_cast<double>(ms) / static_cast<double>(launched[ln]);
+                inflight[ln] = false;
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->wait_s += now_s() - t0;
             }
-            llb_handle h = nullptr;
-            const int hr = rc == LLB_OK ? llb_batch_lattice(s->batch, r->slot, &h) : rc;
-            finish(s, r, h, hr, "batched step");
-            llb_batch_remove(s->batch, r->slot);
+            std::vector<std::shared_ptr<Request>> keep;
+            for (auto& r : s->running[ln]) {
+                if (r->remaining > 0 && rc == LLB_OK) {
+                    keep.push_back(r);
+                    continue;
+                }
+                llb_handle h = nullptr;
+                int dr = llb_batch_detach(b, r->slot, &h);
+                if (dr == LLB_OK) {
+                    r->h = h;
+                    r->rc = rc;
+                } else {
+                    llb_batch_remove(b, r->slot);
+                    r->h = nullptr;
+                    r->rc = dr;
+                }
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->dying.push_back(r);
+                s->cv_reap.notify_all();
+            }
+            s->running[ln].swap(keep);
         }
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->running.swap(keep);
-            s->n_running = static_cast<int64_t>(s->running.size());
+        if (s->running[0].empty() && s->running[1].empty()) continue;
+        // 3. next chunk of each lane, up to the lane's earliest completion; the
+        //    small lane fills the large lane's chunk time
+        int64_t n[2] = {0, 0};
+        for (int ln = 0; ln < 2; ++ln) {
+            if (s->running[ln].empty()) continue;
+            int64_t m = std::numeric_limits<int64_t>::max();
+            for (auto& r : s->running[ln]) m = std::min(m, r->remaining);
+            n[ln] = m;
         }
-        if (s->running.empty()) continue;
-        // 3. next chunk: up to the earliest completion
-        int64_t chunk = s->max_chunk;
-        for (auto& r : s->running) chunk = std::min(chunk, r->remaining);
-        rc = llb_batch_step(s->batch, static_cast<int32_t>(chunk));
-        for (auto& r : s->running) r->remaining -= chunk;
-        if (rc != LLB_OK) {
-            // every running request fails at the next retirement pass
-            for (auto& r : s->running) r->remaining = 0;
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->error = std::string("batched step failed: ") + llb_batch_last_error(s->batch);
+        if (n[1] > 0) n[1] = std::min<int64_t>(n[1], s->max_chunk);
+        if (n[0] > 0) {
+            int64_t cap = s->max_chunk;
+            if (n[1] > 0 && ms_step[0] > 0.0 && ms_step[1] > 0.0)
+                cap = std::max<int64_t>(1, static_cast<int64_t>(n[1] * ms_step[1] / ms_step[0]));
+            n[0] = std::min<int64_t>({n[0], cap, int64_t{1} << 20});
         }
-        inflight = true;
+        for (int ln = 0; ln < 2; ++ln) {
+            if (n[ln] <= 0) continue;
+            llb_batch_handle b = s->batch[ln];
+            int rc = llb_batch_event_record(b, 0);
+            if (rc == LLB_OK) rc = llb_batch_step(b, static_cast<int32_t>(n[ln]));
+            if (rc == LLB_OK) rc = llb_batch_event_record(b, 1);
+            for (auto& r : s->running[ln]) r->remaining -= n[ln];
+            if (rc != LLB_OK) {
+                // every running request of the lane fails at the next retirement pass
+                for (auto& r : s->running[ln]) r->remaining = 0;
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->error = std::string("batched step failed: ") + llb_batch_last_error(b);
+            }
+            inflight[ln] = true;
+            launched[ln] = n[ln];
+        }
         std::lock_guard<std::mutex> lk(s->mu);
         s->chunks += 1;
-        s->batch_steps += chunk;
+        s->batch_steps += n[0] + n[1];
     }
 }
 
@@ -279,20 +382,49 @@ int llb_server_create(int32_t device, int32_t storage, int32_t mode, int64_t bud
     s->mode = mode;
     s->budget = budget_bytes;
     s->max_chunk = max_chunk_steps;
+    auto drop = [&](int rc) {
+        for (auto& c : s->batch)
+            if (c) llb_batch_destroy(c);
+        delete s;
+        return rc;
+    };
     if (mode == LLB_SERVE_BATCHED) {
-        const int rc = llb_batch_create(device, storage, &s->batch);
-        if (rc != LLB_OK) {
-            delete s;
-            return rc;
+        for (auto& b : s->batch) {
+            const int rc = llb_batch_create(device, storage, &b);
+            if (rc != LLB_OK) return drop(rc);
+            llb_batch_set_config(b, 8, 1);
         }
-        llb_batch_set_config(s->batch, 8, 1);
+        // the small lane's blocks go first, so small requests keep their own
+        // step rate beside large lattices
+        llb_batch_set_stream_priority(s->batch[0], std::numeric_limits<int32_t>::min());
     }
     try {
-        s->worker = std::thread(mode == LLB_SERVE_BATCHED ? batched_loop : sequential_loop, s);
+        if (mode == LLB_SERVE_BATCHED) {
+            s->reaper = std::thread(reaper_loop, s);
+            s->worker = std::thread(batched_loop, s);
+            const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+            const int np = static_cast<int>(std::min(4u, std::max(1u, hw / 2)));
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->preparers_live = np;
+            }
+            for (int i = 0; i < np; ++i) s->preparers.emplace_back(preparer_loop, s);
+        } else {
+            s->worker = std::thread(sequential_loop, s);
+        }
     } catch (...) {
-        if (s->batch) llb_batch_destroy(s->batch);
-        delete s;
-        return LLB_E_NOMEM;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stop = s->preparer_done = s->worker_done = true;
+        }
+        s->cv_prep.notify_all();
+        s->cv_work.notify_all();
+        s->cv_reap.notify_all();
+        for (auto& t : s->preparers)
+            if (t.joinable()) t.join();
+        for (std::thread* t : {&s->worker, &s->reaper})
+            if (t->joinable()) t->join();
+        return drop(LLB_E_NOMEM);
     }
     *out = s;
     return LLB_OK;
@@ -309,10 +441,17 @@ int llb_server_destroy(llb_server_handle s) {
         }
         s->queue.clear();
     }
+    s->cv_prep.notify_all();
     s->cv_work.notify_all();
     s->cv_done.notify_all();
-    if (s->worker.joinable()) s->worker.join();
-    if (s->batch) llb_batch_destroy(s->batch);
+    // running requests finish: the preparer stops admitting, the worker drains
+    // its lanes, the reaper retires the last lattices
+    for (auto& t : s->preparers)
+        if (t.joinable()) t.join();
+    for (std::thread* t : {&s->worker, &s->reaper})
+        if (t->joinable()) t->join();
+    for (auto& b : s->batch)
+        if (b) llb_batch_destroy(b);
     delete s;
     return LLB_OK;
 }
@@ -363,7 +502,7 @@ int llb_server_submit(llb_server_handle s, const llb_desc* d, const double* open
     s->all[r->id] = r;
     s->queue.push_back(r);
     *request_id = r->id;
-    s->cv_work.notify_all();
+    s->cv_prep.notify_all();
     return LLB_OK;
 }
 
@@ -423,11 +562,14 @@ int llb_server_stats(llb_server_handle s, llb_server_counters* out) {
     out->failed = s->failed;
     out->node_steps = s->node_steps;
     out->queued = static_cast<int64_t>(s->queue.size());
-    out->running = s->n_running;
+    out->running = s->admitted;
     out->bytes_in_use = s->in_use;
     out->chunks = s->chunks;
     out->batch_steps = s->batch_steps;
     out->clock_s = now_s();
+    out->admit_s = s->admit_s;
+    out->wait_s = s->wait_s;
+    out->retire_s = s->retire_s;
     return LLB_OK;
 }
 

@@ -103,6 +103,8 @@ SIGNATURES = {
     "llb_batch_destroy": [_H],
     "llb_batch_add": [_H, ctypes.POINTER(_Desc), _P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)],
     "llb_batch_remove": [_H, ctypes.c_int32],
+    "llb_batch_attach": [_H, _H, ctypes.POINTER(ctypes.c_int32)],
+    "llb_batch_detach": [_H, ctypes.c_int32, ctypes.POINTER(_H)],
     "llb_batch_step": [_H, ctypes.c_int32],
     "llb_batch_lattice": [_H, ctypes.c_int32, ctypes.POINTER(_H)],
     "llb_batch_set_config": [_H, ctypes.c_int32, ctypes.c_int32],
@@ -111,6 +113,7 @@ SIGNATURES = {
                        ctypes.POINTER(ctypes.c_float)],
     "llb_batch_get_step": [_H, ctypes.POINTER(ctypes.c_int64)],
     "llb_batch_synchronize": [_H],
+    "llb_batch_set_stream_priority": [_H, ctypes.c_int32],
     "llb_batch_event_record": [_H, ctypes.c_int32],
     "llb_batch_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
     "llb_batch_info": [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
@@ -471,7 +474,8 @@ class CudaBatch:
 
 class _ServerCounters(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in ("completed", "failed", "node_steps", "queued", "running",
-                                             "bytes_in_use", "chunks", "batch_steps")] + [("clock_s", ctypes.c_double)]
+                                             "bytes_in_use", "chunks", "batch_steps")] + [(k, ctypes.c_double) for k in ("clock_s", "admit_s", "wait_s",
+                                                                          "retire_s")]
 
 
 def _scheck(rc: int, s):

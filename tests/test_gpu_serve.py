@@ -184,3 +184,40 @@ def test_destroy_with_queued_requests_returns():
     ids = [submit(s, REQS[3]) for _ in range(6)]
     s.close()
     assert len(ids) == 6
+
+
+def test_small_lane_is_not_held_to_the_large_lattices_step_rate():
+    """Lattices of 2^20 nodes or more run in their own lane: a small request
+    with more steps than a large one that runs beside it still finishes
+    first, and both results are bit for bit those of each request alone (and,
+    for the large one, of the plain path)."""
+    import llalbm_cuda as L
+
+    big = ("cavity1024", H.classify(H.cavity_types(1024)), H.Params(tau=0.8), "const:0.05:0", "const:0:0", 10000)
+    small = ("cavity64_long", REQS[0][1], H.Params(tau=0.7), "const:0.08:0", "const:0:0", 12000)
+    alone = {}
+    with L.CudaServer(storage=L.STORE_F64, budget_bytes=8 << 30) as s:
+        for req in (big, small):
+            rid = submit(s, req)
+            s.wait(rid, 300)
+            alone[req[0]] = s.result(rid)
+    with L.CudaServer(storage=L.STORE_F64, mode=L.SERVE_SEQUENTIAL, budget_bytes=8 << 30) as s:
+        rid = submit(s, big)
+        s.wait(rid, 300)
+        plain_big = s.result(rid)
+    with L.CudaServer(storage=L.STORE_F64, budget_bytes=8 << 30) as s:
+        a = submit(s, big)
+        while s.state(a) != L.REQ_RUNNING:
+            time.sleep(0.0005)
+        b = submit(s, small)
+        s.wait(b, 300)
+        s.wait(a, 300)
+        rb, ub, tb = s.result(b)
+        ra, ua, ta = s.result(a)
+    assert tb[2] < ta[2]
+    np.testing.assert_array_equal(ra, alone["cavity1024"][0])
+    np.testing.assert_array_equal(ua, alone["cavity1024"][1])
+    np.testing.assert_array_equal(rb, alone["cavity64_long"][0])
+    np.testing.assert_array_equal(ub, alone["cavity64_long"][1])
+    np.testing.assert_array_equal(ra, plain_big[0])
+    np.testing.assert_array_equal(ua, plain_big[1])
