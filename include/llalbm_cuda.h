@@ -239,6 +239,8 @@ int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, in
 int llb_batch_get_step(llb_batch_handle b, int64_t* step);
 /* Waits for the batch; LLB_E_TIMEOUT if a cooperative launch gave up a grid barrier. */
 int llb_batch_synchronize(llb_batch_handle b);
+/* Without waiting: *done = 1 when everything queued on the batch has run. */
+int llb_batch_query(llb_batch_handle b, int32_t* done);
 /* Scheduling priority of the batch's stream (CUDA stream priorities: a lower
    number is a higher priority; clamped to the device's range, so INT32_MIN
    asks for the highest).  Blocks of a higher-priority stream are scheduled

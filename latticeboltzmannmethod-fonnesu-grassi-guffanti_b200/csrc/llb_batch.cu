@@ -466,6 +466,21 @@ int llb_batch_get_step(llb_batch_handle b, int64_t* step) {
     return LLB_OK;
 }
 
+int llb_batch_query(llb_batch_handle b, int32_t* done) {
+    if (!b || !done) return LLB_E_INVALID;
+    cudaSetDevice(b->device);
+    const cudaError_t e = cudaStreamQuery(b->stream);
+    if (e == cudaSuccess) {
+        *done = 1;
+        return LLB_OK;
+    }
+    if (e == cudaErrorNotReady) {
+        *done = 0;
+        return LLB_OK;
+    }
+    return bfail(b, LLB_E_CUDA, std::string("cudaStreamQuery: ") + cudaGetErrorString(e));
+}
+
 int llb_batch_synchronize(llb_batch_handle b) {
     if (!b) return LLB_E_INVALID;
     cudaSetDevice(b->device);

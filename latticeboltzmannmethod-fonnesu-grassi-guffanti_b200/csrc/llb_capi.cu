@@ -109,28 +109,31 @@ constexpr uint8_t UNSET = 0xff;
 int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vector<uint8_t>& bb,
                std::vector<int32_t>& open_idx, int64_t& n_nonplain, std::string& why) {
     const int64_t R = d->rows, C = d->cols;
-    std::vector<uint8_t> cls(static_cast<size_t>(R * C), UNSET);
+    // provisional codes in a grid with a one-node border of UNSET, so that
+    // neighbour lookups need no bounds checks: 1 fluid, 2 wall/obstacle,
+    // 3 inlet, 4 outlet
+    const int64_t P = R + 2;
+    std::vector<uint8_t> cls(static_cast<size_t>(P * (C + 2)), UNSET);
+    auto cell = [&](int64_t i, int64_t j) -> uint8_t& { return cls[static_cast<size_t>((i + 1) + P * (j + 1))]; };
     auto mark = [&](const int64_t* ij, int64_t n, uint8_t c, const char* name) -> bool {
         if (n > 0 && !ij) { why = std::string(name) + " list is NULL"; return false; }
         for (int64_t q = 0; q < n; ++q) {
             const int64_t i = ij[2 * q], j = ij[2 * q + 1];
             if (i < 0 || j < 0 || i >= R || j >= C) { why = std::string(name) + " node out of range"; return false; }
-            uint8_t& s = cls[static_cast<size_t>(i + R * j)];
+            uint8_t& s = cell(i, j);
             if (s != UNSET) { why = std::string(name) + " node also listed as another node kind"; return false; }
             s = c;
         }
         return true;
     };
-    // provisional codes: 1 fluid, 2 wall/obstacle, 3 inlet, 4 outlet
     if (!mark(d->fluid_ij, d->n_fluid, 1, "fluid") || !mark(d->wall_ij, d->n_wall, 2, "wall") ||
         !mark(d->inlet_ij, d->n_inlet, 3, "inlet") || !mark(d->outlet_ij, d->n_outlet, 4, "outlet") ||
         !mark(d->obstacle_ij, d->n_obstacle, 2, "obstacle"))
         return LLB_E_GEOMETRY;
-    auto at = [&](int64_t i, int64_t j) -> uint8_t {
-        if (i < 0 || j < 0 || i >= R || j >= C) return UNSET;
-        return cls[static_cast<size_t>(i + R * j)];
-    };
     auto active = [](uint8_t c) { return c == 1 || c == 3 || c == 4; };
+    // offset in the bordered grid of the source x - c_k of direction k
+    int64_t src_off[9];
+    for (int k = 0; k < 9; ++k) src_off[k] = -(DI(k) + P * DJ(k));
     // The reference streams fluid nodes without bounds checks; a fluid node on
     // the lattice edge would write outside its tensors.
     for (int64_t q = 0; q < d->n_fluid; ++q) {
@@ -144,9 +147,10 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
     if (d->obstacle_dirs) {
         for (int64_t q = 0; q < d->n_obstacle; ++q) {
             const int64_t i = d->obstacle_ij[2 * q], j = d->obstacle_ij[2 * q + 1];
+            const uint8_t* x = &cell(i, j);
             uint16_t b = 0;
             for (int k = 1; k < 9; ++k)
-                if (active(at(i + DI(k), j + DJ(k)))) b |= static_cast<uint16_t>(1u << k);
+                if (active(x[-src_off[k]])) b |= static_cast<uint16_t>(1u << k);
             if (b != (d->obstacle_dirs[q] & 0x1feu)) {
                 why = "obstacle direction bits differ from the neighbour rule of identify_obstacle_propagation";
                 return LLB_E_UNSUPPORTED;
@@ -158,27 +162,29 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
     bb.assign(static_cast<size_t>(ld) * C, 0);
     open_idx.assign(static_cast<size_t>(ld) * C, -1);
     auto side_code = [](int32_t bt) { return (bt >= 1 && bt <= 4) ? bt : SIDE_NONE; };
+    static constexpr uint8_t kClass[5] = {CLS_DEAD, CLS_FLUID, CLS_BB, CLS_OPEN, CLS_OPEN};
     for (int64_t j = 0; j < C; ++j) {
+        const uint8_t* col = &cell(0, j);
+        uint8_t* mcol = mask.data() + static_cast<size_t>(j * ld);
+        uint8_t* bcol = bb.data() + static_cast<size_t>(j * ld);
         for (int64_t i = 0; i < R; ++i) {
-            const uint8_t c = at(i, j);
-            uint8_t m = CLS_DEAD;
-            if (c == 1) m = CLS_FLUID;
-            else if (c == 2) m = CLS_BB;
-            else if (c == 3 || c == 4) m = CLS_OPEN;
-            uint8_t b = 0;
+            const uint8_t c = col[i];
+            if (c == UNSET) continue;  // dead: mask and bounce bits stay 0
+            uint8_t m = kClass[c];
             if (active(c)) {
+                const uint8_t* x = col + i;
                 bool plain = true;
+                uint8_t b = 0;
                 for (int k = 1; k < 9; ++k) {
-                    const int64_t si = i - DI(k), sj = j - DJ(k);
-                    const uint8_t s = at(si, sj);
-                    if (!active(s)) plain = false;
-                    if (s == 2) b |= static_cast<uint8_t>(1u << (k - 1));
+                    const uint8_t sk = x[src_off[k]];
+                    plain &= active(sk);
+                    b |= static_cast<uint8_t>((sk == 2) << (k - 1));
                 }
                 if (plain) m |= MASK_PLAIN;
                 else ++n_nonplain;
+                bcol[i] = b;
             }
-            mask[static_cast<size_t>(j * ld + i)] = m;
-            bb[static_cast<size_t>(j * ld + i)] = b;
+            mcol[i] = m;
         }
     }
     auto set_open = [&](const int64_t* ij, const int32_t* side, int64_t n, int bc, int base) {

@@ -39,9 +39,9 @@ cudaError_t launch_gather_forces_lowp(int storage, const LaunchCtx& x, const voi
 }
 
 // TMA pipeline configurations (tile rows, tile columns, stages, consumer warps)
-using F32Cfg0 = TmaCfg<float, 128, 16, 2, 16>;
-using F32Cfg1 = TmaCfg<float, 128, 8, 4, 24>;
-using F32Cfg2 = TmaCfg<float, 128, 12, 3, 24>;
+using F32Cfg0 = TmaCfg<float, 128, 8, 3, 16>;
+using F32Cfg1 = TmaCfg<float, 128, 16, 2, 16>;
+using F32Cfg2 = TmaCfg<float, 128, 8, 4, 24>;
 using F16Cfg0 = TmaCfg<__half, 128, 24, 3, 24>;
 using F16Cfg1 = TmaCfg<__half, 128, 16, 3, 16>;
 using F16Cfg2 = TmaCfg<__half, 128, 32, 2, 16>;

@@ -9,13 +9,13 @@
 //  * the worker moves prepared lattices into one of two lanes, each a batch on
 //    its own stream -- lattices of fewer than 2^20 nodes share the work-list
 //    kernel (small lane), larger ones are stepped by their own launches (large
-//    lane) -- and advances the lanes chunk by chunk.  The lanes run
-//    concurrently; the small lane's stream has the higher scheduling priority,
-//    so a small request keeps its own step rate beside large lattices.  Each
-//    chunk the large lane runs at most max_chunk steps and the small lane as
-//    many steps as fit in the same time (measured per-step times), each never
-//    past its earliest completion; prepared lattices join at the next chunk
-//    boundary, so their work overlaps the work already running;
+//    lane) -- and advances each lane chunk by chunk, at most max_chunk steps
+//    and never past the lane's earliest completion.  The lanes run
+//    concurrently and independently: a lane whose chunk is done is drained
+//    and relaunched at once while the other runs on.  The small lane's stream
+//    has the higher scheduling priority, so a small request keeps its own step
+//    rate beside large lattices.  Prepared lattices join at their lane's next
+//    chunk boundary, so their work overlaps the work already running;
 //  * the reaper takes finished lattices out of the worker's way, copies their
 //    result -- the rho and u the reference's Lattice holds after
 //    perform_lbm(steps) -- to host memory and frees them, which returns their
@@ -254,10 +254,57 @@ void reaper_loop(llb_server_handle s) {
     }
 }
 
+// Waits for a lane's chunk, measures it, hands what it finished to the reaper.
+void drain_lane(llb_server_handle s, int ln) {
+    llb_batch_handle b = s->batch[ln];
+    const double t0 = now_s();
+    const int rc = llb_batch_synchronize(b);
+    std::vector<std::shared_ptr<Request>> keep;
+    for (auto& r : s->running[ln]) {
+        if (r->remaining > 0 && rc == LLB_OK) {
+            keep.push_back(r);
+            continue;
+        }
+        llb_handle h = nullptr;
+        const int dr = llb_batch_detach(b, r->slot, &h);
+        if (dr == LLB_OK) {
+            r->h = h;
+            r->rc = rc;
+        } else {
+            llb_batch_remove(b, r->slot);
+            r->h = nullptr;
+            r->rc = dr;
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->dying.push_back(r);
+        s->cv_reap.notify_all();
+    }
+    s->running[ln].swap(keep);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->wait_s += now_s() - t0;
+}
+
+// Next chunk of a lane: at most max_chunk steps, never past its earliest completion.
+void launch_lane(llb_server_handle s, int ln) {
+    llb_batch_handle b = s->batch[ln];
+    int64_t n = s->max_chunk;
+    for (auto& r : s->running[ln]) n = std::min(n, r->remaining);
+    const int rc = llb_batch_step(b, static_cast<int32_t>(n));
+    for (auto& r : s->running[ln]) r->remaining -= n;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (rc != LLB_OK) {
+        // every running request of the lane fails at its next drain
+        for (auto& r : s->running[ln]) r->remaining = 0;
+        s->error = std::string("batched step failed: ") + llb_batch_last_error(b);
+    }
+    s->chunks += 1;
+    s->batch_steps += n;
+}
+
+// The lanes are independent: whichever lane's chunk has finished is drained
+// and relaunched at once, while the other lane keeps running.
 void batched_loop(llb_server_handle s) {
-    bool inflight[2] = {false, false};  // a chunk was launched on the lane and not yet waited for
-    int64_t launched[2] = {0, 0};       // steps of that chunk
-    double ms_step[2] = {0.0, 0.0};     // measured device time per step (0: not measured yet)
+    bool inflight[2] = {false, false};  // a chunk was launched on the lane and not yet drained
     for (;;) {
         const bool idle = s->running[0].empty() && s->running[1].empty() && !inflight[0] && !inflight[1];
         std::deque<std::shared_ptr<Request>> joining;
@@ -271,7 +318,8 @@ void batched_loop(llb_server_handle s) {
             }
             joining.swap(s->ready);
         }
-        // 1. prepared lattices join their lane (step 0 queued on the lane's stream)
+        // 1. prepared lattices join their lane (step 0 queued on the lane's stream,
+        //    behind a chunk in flight)
         for (auto& r : joining) {
             const int ln = lane_of(*r);
             int32_t slot = -1;
@@ -287,78 +335,28 @@ void batched_loop(llb_server_handle s) {
             r->remaining = r->steps - 2;  // step 0 was the first collision
             s->running[ln].push_back(r);
         }
-        // 2. per lane: wait for the chunk in flight, hand what it finished to the reaper
+        // 2. every lane whose chunk is done (or that has none): drain, relaunch
+        bool progressed = !joining.empty();
         for (int ln = 0; ln < 2; ++ln) {
-            llb_batch_handle b = s->batch[ln];
-            int rc = LLB_OK;
             if (inflight[ln]) {
-                const double t0 = now_s();
-                rc = llb_batch_synchronize(b);
-                float ms = 0.f;
-                if (rc == LLB_OK && launched[ln] > 0 && llb_batch_event_elapsed_ms(b, 0, 1, &ms) == LLB_OK)
-                    ms_step[ln] = static_cast<double>(ms) / static_cast<double>(launched[ln]);
+                int32_t done = 0;
+                if (llb_batch_query(s->batch[ln], &done) == LLB_OK && !done) continue;
                 inflight[ln] = false;
-                std::lock_guard<std::mutex> lk(s->mu);
-                s->wait_s += now_s() - t0;
+                progressed = true;
+            } else if (s->running[ln].empty()) {
+                continue;
             }
-            std::vector<std::shared_ptr<Request>> keep;
-            for (auto& r : s->running[ln]) {
-                if (r->remaining > 0 && rc == LLB_OK) {
-                    keep.push_back(r);
-                    continue;
-                }
-                llb_handle h = nullptr;
-                int dr = llb_batch_detach(b, r->slot, &h);
-                if (dr == LLB_OK) {
-                    r->h = h;
-                    r->rc = rc;
-                } else {
-                    llb_batch_remove(b, r->slot);
-                    r->h = nullptr;
-                    r->rc = dr;
-                }
-                std::lock_guard<std::mutex> lk(s->mu);
-                s->dying.push_back(r);
-                s->cv_reap.notify_all();
-            }
-            s->running[ln].swap(keep);
-        }
-        if (s->running[0].empty() && s->running[1].empty()) continue;
-        // 3. next chunk of each lane, up to the lane's earliest completion; the
-        //    small lane fills the large lane's chunk time
-        int64_t n[2] = {0, 0};
-        for (int ln = 0; ln < 2; ++ln) {
+            drain_lane(s, ln);
             if (s->running[ln].empty()) continue;
-            int64_t m = std::numeric_limits<int64_t>::max();
-            for (auto& r : s->running[ln]) m = std::min(m, r->remaining);
-            n[ln] = m;
-        }
-        if (n[1] > 0) n[1] = std::min<int64_t>(n[1], s->max_chunk);
-        if (n[0] > 0) {
-            int64_t cap = s->max_chunk;
-            if (n[1] > 0 && ms_step[0] > 0.0 && ms_step[1] > 0.0)
-                cap = std::max<int64_t>(1, static_cast<int64_t>(n[1] * ms_step[1] / ms_step[0]));
-            n[0] = std::min<int64_t>({n[0], cap, int64_t{1} << 20});
-        }
-        for (int ln = 0; ln < 2; ++ln) {
-            if (n[ln] <= 0) continue;
-            llb_batch_handle b = s->batch[ln];
-            int rc = llb_batch_event_record(b, 0);
-            if (rc == LLB_OK) rc = llb_batch_step(b, static_cast<int32_t>(n[ln]));
-            if (rc == LLB_OK) rc = llb_batch_event_record(b, 1);
-            for (auto& r : s->running[ln]) r->remaining -= n[ln];
-            if (rc != LLB_OK) {
-                // every running request of the lane fails at the next retirement pass
-                for (auto& r : s->running[ln]) r->remaining = 0;
-                std::lock_guard<std::mutex> lk(s->mu);
-                s->error = std::string("batched step failed: ") + llb_batch_last_error(b);
-            }
+            launch_lane(s, ln);
             inflight[ln] = true;
-            launched[ln] = n[ln];
+            progressed = true;
         }
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->chunks += 1;
-        s->batch_steps += n[0] + n[1];
+        if (!progressed) {
+            // both lanes busy: doze until a prepared lattice arrives or a moment passes
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait_for(lk, std::chrono::microseconds(200), [&] { return !s->ready.empty(); });
+        }
     }
 }
 

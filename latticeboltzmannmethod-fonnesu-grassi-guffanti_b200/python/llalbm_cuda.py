@@ -113,6 +113,7 @@ SIGNATURES = {
                        ctypes.POINTER(ctypes.c_float)],
     "llb_batch_get_step": [_H, ctypes.POINTER(ctypes.c_int64)],
     "llb_batch_synchronize": [_H],
+    "llb_batch_query": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_batch_set_stream_priority": [_H, ctypes.c_int32],
     "llb_batch_event_record": [_H, ctypes.c_int32],
     "llb_batch_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
