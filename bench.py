@@ -465,7 +465,7 @@ def run_batch(a, dist):
     path."""
     import llalbm_cuda as L
 
-    probs = W.batch_problems()
+    probs = W.batch_problems()[:a.lattices]
     nodes = sum(p["rows"] * p["cols"] for p in probs)
     b = L.CudaBatch(storage=L.STORE_F32S, device=dist.local)
     active = 0
@@ -508,7 +508,7 @@ def run_batch(a, dist):
         "metric": METRIC, "value": round(batched, 1), "unit": "MLUPS", "n_gpus": dist.world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(per, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (shifted storage)", "data": "synthetic",
-        "config": {"workload": "batch256", "lattices": len(probs), "nodes": nodes, "active_nodes": active,
+        "config": {"workload": "batch256" if len(probs) == 256 else f"batch256[:{len(probs)}]", "lattices": len(probs), "nodes": nodes, "active_nodes": active,
                    "description": "256 problems, nx 64..1024 step 32, aspect 1..4, half lid cavities, half "
                                   "channels with 0-8 discs, tau U[0.55,1.5], BGK/TRT 50/50",
                    "launch": {"block_y": by, "steps_per_launch": spl, "autotuned_ms_per_step": round(tune_ms, 4)}},
@@ -694,6 +694,8 @@ def main():
     ap.add_argument("--pipeline", type=int, default=None,
                     help="plain path step kernel: -1 one thread per node, 0..2 TMA configurations (default: per lattice)")
     ap.add_argument("--launch-shape", type=int, default=None, help="columns per block of the one-thread kernel")
+    ap.add_argument("--lattices", type=int, default=256,
+                    help="batch256 workload: the first N of the 256 problems (smaller batches for profiling)")
     ap.add_argument("--requests", type=int, default=96, help="requests in the served stream (workload serve)")
     ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous and cavity workloads")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
