@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define LLB_ABI_VERSION 1
+#define LLB_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define LLB_OK 0
@@ -62,6 +62,11 @@ extern "C" {
 #define LLB_BC_ZH_VELOCITY 0
 #define LLB_BC_OPEN 1
 #define LLB_BC_ZH_PRESSURE 2
+/* obstacle policies: BounceBackPolicy (boundaries/BounceBackPolicy.hpp:143-187)
+   and PSBounceBackPolicy, partially saturated bounce-back
+   (boundaries/PSBounceBackPolicy.hpp:177-293; FP64 storage, single lattices) */
+#define LLB_OBSTACLE_BOUNCE_BACK 0
+#define LLB_OBSTACLE_PARTIAL 1
 /* InputNodeType codes of the lattice file format (aliases.hpp:41-48) */
 #define LLB_NODE_FLUID 0
 #define LLB_NODE_SOLID 1
@@ -93,6 +98,9 @@ typedef struct {
     int32_t pattern;                                      /* LLB_PATTERN_* */
     int32_t device;                                       /* CUDA ordinal */
     int32_t open_table_rows;  /* per-step open-value ring capacity; 1 = values constant in time */
+    int32_t obstacle_bc;                                  /* LLB_OBSTACLE_* (0: bounce-back) */
+    double ps_tau;                                        /* PSBounceBackPolicy<2>::tau */
+    const double* obstacle_b;  /* per wet obstacle, ObstaclePoint::get_b(); NULL: 1.0 (its default) */
 } llb_desc;
 
 /* Node vectors as the reference builds them from a grid of InputNodeType codes. */
@@ -197,6 +205,40 @@ int llb_flow_forces_noalloc(llb_handle h, const int64_t* ij, const uint16_t* dir
    inlet and outlet nodes of sum_k f, c_x f, c_y f) with compensated FP64;
    out[0] = mass, out[1] = momentum along j (u_x), out[2] = along -i (u_y). */
 int llb_mass_momentum(llb_handle h, double out[3]);
+
+/* ---- output writer ------------------------------------------------------- */
+/* Writes the reference's velocity output files off the stepping thread:
+   util::writer::write_lattice_file<2> (utils/writers/LatticeWriter.hpp:60-92),
+   called by perform_lbm on save steps (Lattice.hpp:370-374), creates
+   <dir>/output-<n>u_x.txt and <dir>/output-<n>u_y.txt with one text row per
+   lattice row i holding u(i, j, d) for j = 0..C-1, each value in std::ostream's
+   default format (printf "%.6g") followed by a space.  The files here are
+   byte-identical.
+
+   llb_writer_save_u enqueues, on the lattice's stream, a copy of u (written by
+   the last LLB_STEP_MACRO step) into one of `slots` pinned host buffers and
+   returns; the next steps may be enqueued at once (they run after the copy on
+   the same stream).  A writer thread waits for the copy, formats the rows on
+   `threads` threads and writes both files.  A call blocks only while every
+   slot is still being written.  Errors of the background work (a file that
+   cannot be opened, a CUDA error) are returned by the next save, by
+   llb_writer_flush and by llb_writer_destroy.  The directory must exist.  One
+   writer serves one calling thread at a time; flush (or destroy) the writer
+   before destroying a lattice whose copies are still queued. */
+typedef struct llb_writer* llb_writer_handle;
+/* slots in [1, 64] (0: 3); threads in [1, 256] (0: up to 8 host threads). */
+int llb_writer_create(const char* dir, int32_t slots, int32_t threads, llb_writer_handle* out);
+int llb_writer_save_u(llb_writer_handle w, llb_handle h, int64_t index);
+/* The same files from a host array u in the reference's (R, C, 2) column-major
+   layout; u is copied before the call returns. */
+int llb_writer_save_host(llb_writer_handle w, const double* u, int64_t rows, int64_t cols, int64_t index);
+/* Waits until every queued file is written. */
+int llb_writer_flush(llb_writer_handle w);
+/* Files written so far and the seconds the writer thread spent waiting for
+   copies and formatting/writing. */
+int llb_writer_stats(llb_writer_handle w, int64_t* files, double* wait_s, double* write_s);
+int llb_writer_destroy(llb_writer_handle w);
+const char* llb_writer_last_error(llb_writer_handle w);
 
 /* ---- batches of lattices ------------------------------------------------ */
 /* Many independent lattices (uneven sizes, BGK or TRT, own relaxation times,

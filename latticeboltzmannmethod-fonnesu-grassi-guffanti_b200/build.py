@@ -32,6 +32,7 @@ SOURCES = {
     "llb_batch.cu": [],
     "llb_server.cpp": [],
     "llb_classify.cpp": [],
+    "llb_writer.cpp": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(INCLUDE, "llalbm_cuda.h")

@@ -312,6 +312,7 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
     if (h->storage != b->storage || h->pattern != LLB_PATTERN_AB || h->device != b->device)
         return bfail(b, LLB_E_INVALID, "lattice storage, pattern or device differs from the batch");
     if (!h->own_stream) return bfail(b, LLB_E_STATE, "lattice already belongs to a batch");
+    if (h->d_ps) return bfail(b, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the single-lattice path");
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
     // the lattice works on the batch's stream from now on
     LLB_BCUDA(b, cudaStreamSynchronize(h->stream));

@@ -70,6 +70,8 @@ LaunchCtx make_ctx(llb_handle h) {
     x.g.plane = h->plane;
     x.g.mask = h->d_mask;
     x.g.bb = h->d_bb;
+    x.g.ps = h->d_ps;
+    x.g.psb = h->d_psb;
     x.g.open_idx = h->d_open_idx;
     x.ot.vals = h->d_open;
     x.ot.n_open = h->n_open;
@@ -91,7 +93,7 @@ void release(llb_handle h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& g : h->graph)
         if (g) cudaGraphExecDestroy(g);
-    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
+    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_ps, h->d_psb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
                     h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -107,11 +109,13 @@ void release(llb_handle h) {
 constexpr uint8_t UNSET = 0xff;
 
 int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vector<uint8_t>& bb,
-               std::vector<int32_t>& open_idx, int64_t& n_nonplain, std::string& why) {
+               std::vector<uint8_t>& ps, std::vector<double>& psb, std::vector<int32_t>& open_idx,
+               int64_t& n_nonplain, std::string& why) {
     const int64_t R = d->rows, C = d->cols;
+    const bool partial = d->obstacle_bc == LLB_OBSTACLE_PARTIAL;
     // provisional codes in a grid with a one-node border of UNSET, so that
     // neighbour lookups need no bounds checks: 1 fluid, 2 wall/obstacle,
-    // 3 inlet, 4 outlet
+    // 3 inlet, 4 outlet, 5 partially saturated obstacle
     const int64_t P = R + 2;
     std::vector<uint8_t> cls(static_cast<size_t>(P * (C + 2)), UNSET);
     auto cell = [&](int64_t i, int64_t j) -> uint8_t& { return cls[static_cast<size_t>((i + 1) + P * (j + 1))]; };
@@ -128,7 +132,7 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
     };
     if (!mark(d->fluid_ij, d->n_fluid, 1, "fluid") || !mark(d->wall_ij, d->n_wall, 2, "wall") ||
         !mark(d->inlet_ij, d->n_inlet, 3, "inlet") || !mark(d->outlet_ij, d->n_outlet, 4, "outlet") ||
-        !mark(d->obstacle_ij, d->n_obstacle, 2, "obstacle"))
+        !mark(d->obstacle_ij, d->n_obstacle, partial ? 5 : 2, "obstacle"))
         return LLB_E_GEOMETRY;
     auto active = [](uint8_t c) { return c == 1 || c == 3 || c == 4; };
     // offset in the bordered grid of the source x - c_k of direction k
@@ -161,8 +165,17 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
     mask.assign(static_cast<size_t>(ld) * C, 0);
     bb.assign(static_cast<size_t>(ld) * C, 0);
     open_idx.assign(static_cast<size_t>(ld) * C, -1);
+    if (partial) {
+        ps.assign(static_cast<size_t>(ld) * C, 0);
+        psb.assign(static_cast<size_t>(ld) * C, 1.0);
+        for (int64_t q = 0; q < d->n_obstacle; ++q) {
+            const double b = d->obstacle_b ? d->obstacle_b[q] : 1.0;
+            if (!(b >= 0.0 && b <= 1.0)) { why = "obstacle b outside [0, 1]"; return LLB_E_INVALID; }
+            psb[static_cast<size_t>(d->obstacle_ij[2 * q + 1] * ld + d->obstacle_ij[2 * q])] = b;
+        }
+    }
     auto side_code = [](int32_t bt) { return (bt >= 1 && bt <= 4) ? bt : SIDE_NONE; };
-    static constexpr uint8_t kClass[5] = {CLS_DEAD, CLS_FLUID, CLS_BB, CLS_OPEN, CLS_OPEN};
+    static constexpr uint8_t kClass[6] = {CLS_DEAD, CLS_FLUID, CLS_BB, CLS_OPEN, CLS_OPEN, CLS_BB};
     for (int64_t j = 0; j < C; ++j) {
         const uint8_t* col = &cell(0, j);
         uint8_t* mcol = mask.data() + static_cast<size_t>(j * ld);
@@ -174,15 +187,17 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
             if (active(c)) {
                 const uint8_t* x = col + i;
                 bool plain = true;
-                uint8_t b = 0;
+                uint8_t b = 0, p = 0;
                 for (int k = 1; k < 9; ++k) {
                     const uint8_t sk = x[src_off[k]];
                     plain &= active(sk);
                     b |= static_cast<uint8_t>((sk == 2) << (k - 1));
+                    p |= static_cast<uint8_t>((sk == 5) << (k - 1));
                 }
                 if (plain) m |= MASK_PLAIN;
                 else ++n_nonplain;
                 bcol[i] = b;
+                if (partial) ps[static_cast<size_t>(j * ld + i)] = p;
             }
             mcol[i] = m;
         }
@@ -412,6 +427,13 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     if (d->collision == LLB_BGK && !(d->tau > 0.0)) return fail(nullptr, LLB_E_INVALID, "tau must be > 0");
     if (d->collision == LLB_TRT && !(d->tau_even > 0.0 && d->tau_odd > 0.0))
         return fail(nullptr, LLB_E_INVALID, "tau_even and tau_odd must be > 0");
+    if (d->obstacle_bc != LLB_OBSTACLE_BOUNCE_BACK && d->obstacle_bc != LLB_OBSTACLE_PARTIAL)
+        return fail(nullptr, LLB_E_INVALID, "bad obstacle policy");
+    if (d->obstacle_bc == LLB_OBSTACLE_PARTIAL) {
+        if (!(d->ps_tau > 0.0)) return fail(nullptr, LLB_E_INVALID, "ps_tau must be > 0");
+        if (d->storage != LLB_STORE_F64)
+            return fail(nullptr, LLB_E_UNSUPPORTED, "partially saturated obstacles need FP64 storage");
+    }
     const int64_t n_open = d->n_inlet + d->n_outlet;
     if (n_open > (1LL << 30)) return fail(nullptr, LLB_E_INVALID, "too many open nodes");
     const int cap = d->open_table_rows <= 0 ? 1 : d->open_table_rows;
@@ -444,16 +466,19 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     h->coll.ief = static_cast<float>(h->coll.ie);
     h->coll.hef = static_cast<float>(h->coll.he);
     h->coll.hof = static_cast<float>(h->coll.ho);
+    if (d->obstacle_bc == LLB_OBSTACLE_PARTIAL) h->coll.ps_t = 1.0 / d->ps_tau;  // PSBounceBackPolicy.hpp:200
 
-    std::vector<uint8_t> mask, bb;
+    std::vector<uint8_t> mask, bb, ps;
+    std::vector<double> psb;
     std::vector<int32_t> open_idx;
     std::string why;
-    int rc = build_mask(d, h->ld, mask, bb, open_idx, h->n_nonplain, why);
+    int rc = build_mask(d, h->ld, mask, bb, ps, psb, open_idx, h->n_nonplain, why);
     if (rc != LLB_OK) { delete h; return fail(nullptr, rc, why); }
     h->n_active = d->n_fluid + d->n_inlet + d->n_outlet;
     // default kernel: pipeline configuration 1 (FP64) or 0 (shifted forms), the
     // fastest measured on the 4096^2 porous channel, or one thread per node
     h->tma_cfg = prefers_tma(*h) ? (d->storage == LLB_STORE_F64 ? 1 : 0) : -1;
+    if (!ps.empty()) h->tma_cfg = -1;  // partially saturated obstacles: one thread per node only
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete h; return fail(nullptr, LLB_E_NODEVICE, "no CUDA device"); }
@@ -474,7 +499,13 @@ int llb_create(const llb_desc* d, llb_handle* out) {
         (rc = dev_alloc(h, &h->d_rho, sizeof(double) * N)) || (rc = dev_alloc(h, &h->d_u, sizeof(double) * 2 * N)) ||
         (rc = dev_alloc(h, &h->d_step, sizeof(long long))) || (rc = dev_alloc(h, &h->d_flags, sizeof(unsigned))) || (rc = dev_alloc(h, &h->d_red, sizeof(double) * 4)))
         return bail(rc);
+    if (!ps.empty() && ((rc = dev_alloc(h, &h->d_ps, ps.size())) || (rc = dev_alloc(h, &h->d_psb, psb.size() * sizeof(double)))))
+        return bail(rc);
     e = cudaMemcpyAsync(h->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && h->d_ps)
+        e = cudaMemcpyAsync(h->d_ps, ps.data(), ps.size(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && h->d_psb)
+        e = cudaMemcpyAsync(h->d_psb, psb.data(), psb.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_bb, bb.data(), bb.size(), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(h->d_open_idx, open_idx.data(), open_idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
@@ -723,6 +754,8 @@ int llb_event_elapsed_ms(llb_handle h, int32_t a, int32_t b, float* ms) {
 
 int llb_set_pipeline(llb_handle h, int32_t config) {
     if (!h || config < -1 || config >= TMA_CONFIGS) return fail(h, LLB_E_INVALID, "config must be -1 or in [0, 3)");
+    if (config >= 0 && h->d_ps)
+        return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
     if (config != h->tma_cfg) {
         int rc = select_device(h);
         if (rc) return rc;

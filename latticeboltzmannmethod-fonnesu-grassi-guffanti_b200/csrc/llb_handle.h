@@ -28,6 +28,8 @@ struct llb_lattice {
     int cur = 0;
     uint8_t* d_mask = nullptr;
     uint8_t* d_bb = nullptr;
+    uint8_t* d_ps = nullptr;   // partially saturated obstacles only
+    double* d_psb = nullptr;
     int32_t* d_open_idx = nullptr;
     double2* d_open = nullptr;
     int n_open = 0, cap = 1;

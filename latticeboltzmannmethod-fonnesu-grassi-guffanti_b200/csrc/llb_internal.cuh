@@ -78,6 +78,10 @@ struct Geometry {
     long long plane;    // ld * cols
     const uint8_t* __restrict__ mask;
     const uint8_t* __restrict__ bb;       // bounce bits
+    // partially saturated obstacles (NULL otherwise): bit k - 1 set when the
+    // source of direction k is such an obstacle; its b per node
+    const uint8_t* __restrict__ ps;
+    const double* __restrict__ psb;
     const int32_t* __restrict__ open_idx;
 };
 
@@ -95,6 +99,8 @@ struct Collision {
     double ie, he, ho;
     // the same rates rounded to FP32 for the shifted storage forms
     float tf, omtf, ief, hef, hof;
+    // partially saturated obstacles: 1/tau of PSBounceBackPolicy (PSBounceBackPolicy.hpp:200)
+    double ps_t;
 };
 
 struct MacroOut {

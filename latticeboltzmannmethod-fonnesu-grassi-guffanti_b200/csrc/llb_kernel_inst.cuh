@@ -16,6 +16,21 @@ cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, 
     const T* in = static_cast<const T*>(fin);
     T* out = static_cast<T*>(fout);
 #define LLB_STEP(COLL, MAC, INI) k_step<M, COLL, MAC, INI><<<grid, block, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss)
+#define LLB_STEP_PS(COLL, MAC, INI) \
+    k_step<M, COLL, MAC, INI, true><<<grid, block, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss)
+    if constexpr (std::is_same_v<M, ModelF64>) {
+        if (x.g.ps) {  // partially saturated obstacles
+            if (x.c.model == 0) {
+                if (init) { if (macro) LLB_STEP_PS(0, true, true); else LLB_STEP_PS(0, false, true); }
+                else { if (macro) LLB_STEP_PS(0, true, false); else LLB_STEP_PS(0, false, false); }
+            } else {
+                if (init) { if (macro) LLB_STEP_PS(1, true, true); else LLB_STEP_PS(1, false, true); }
+                else { if (macro) LLB_STEP_PS(1, true, false); else LLB_STEP_PS(1, false, false); }
+            }
+            return cudaGetLastError();
+        }
+    }
+#undef LLB_STEP_PS
     if (x.c.model == 0) {
         if (init) { if (macro) LLB_STEP(0, true, true); else LLB_STEP(0, false, true); }
         else { if (macro) LLB_STEP(0, true, false); else LLB_STEP(0, false, false); }

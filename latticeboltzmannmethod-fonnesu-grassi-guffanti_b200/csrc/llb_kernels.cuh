@@ -114,9 +114,55 @@ __device__ __forceinline__ bool sector_has_active(bool active) {
     return (ballot & group) != 0u;
 }
 
+// Partially saturated obstacles (PSBounceBackPolicy<2>, PSBounceBackPolicy.hpp:177-293).
+// The reference, after streaming, rewrites for every wet obstacle x and every
+// direction k whose neighbour x_f = x + c_k is fluid or open the population
+// x_f receives from x:
+//   pop(x_f, k) = p - (1 - b)(p - e_opp) t + b ((pop(x_f, k) - e_k) - (p - w_k rho_x)),
+//   p = f*(x_f, opp k) (streamed into x), e from x_f's rho and u of the step,
+//   rho_x = 1 (global_rho of an obstacle is never updated), t = 1 / tau_ps.
+// Every term is known to x_f at the end of its own step, so x_f computes the
+// value and writes it into the obstacle's (otherwise unused) slot (x, k);
+// next step's pull reads it there as from any source.  The equilibria are the
+// policy's own expressions, evaluated in its order.
+__device__ __forceinline__ double ps_equilibrium(int k, double rho, double ux, double uy) {
+    constexpr double one18 = (1.0 / 18.0);
+    constexpr double one36 = (1.0 / 36.0);
+    const double u2 = ux * ux + uy * uy;
+    switch (k) {
+    case 1: return one18 * rho * (2 + 6 * ux + 9 * ux * ux - 3 * u2);
+    case 3: return one18 * rho * (2 - 6 * ux + 9 * ux * ux - 3 * u2);
+    case 2: return one18 * rho * (2 + 6 * uy + 9 * uy * uy - 3 * u2);
+    case 4: return one18 * rho * (2 - 6 * uy + 9 * uy * uy - 3 * u2);
+    case 5: return one36 * rho * (1 + 3 * (ux + uy) + 9 * ux * uy + 3 * u2);
+    case 7: return one36 * rho * (1 - 3 * (ux + uy) + 9 * ux * uy + 3 * u2);
+    case 6: return one36 * rho * (1 - 3 * (ux - uy) - 9 * ux * uy + 3 * u2);
+    default: return one36 * rho * (1 + 3 * (ux - uy) - 9 * ux * uy + 3 * u2);
+    }
+}
+
+// s: the node's populations before collision, f: after; bits: ps bits of the node.
+template <typename T>
+__device__ __forceinline__ void ps_push(const Geometry& g, T* __restrict__ fout, long long node, unsigned bits,
+                                        const double* s, const double* f, double rho, double ux, double uy, double t) {
+    constexpr double one18 = (1.0 / 18.0);
+    constexpr double one36 = (1.0 / 36.0);
+#pragma unroll
+    for (int k = 1; k < 9; ++k) {
+        if (!((bits >> (k - 1)) & 1u)) continue;
+        const long long x = node - (DJ(k) * g.ld + DI(k));  // the obstacle
+        const double b = g.psb[x];
+        const double p = f[opp(k)];
+        const double ek = ps_equilibrium(k, rho, ux, uy);
+        const double eo = ps_equilibrium(opp(k), rho, ux, uy);
+        const double wr = k <= 4 ? 2 * one18 * 1.0 : one36 * 1.0;
+        fout[k * g.plane + x] = p - (1.0 - b) * (p - eo) * t + b * ((s[k] - ek) - (p - wr));
+    }
+}
+
 // INIT == true: step 0 from the initial equilibrium (Lattice.hpp:326-328).
 // Block: 32 rows (one warp per column) x blockDim.y columns, blockDim.y <= BY.
-template <class M, int COLL, bool MACRO, bool INIT>
+template <class M, int COLL, bool MACRO, bool INIT, bool PS = false>
 __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Collision c,
                                                  const typename M::T* __restrict__ fin,
                                                  typename M::T* __restrict__ fout, MacroOut mo, StepSync ss) {
@@ -158,11 +204,22 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
                 mo.u[d] = xr;
                 mo.u[d + N] = yr;
             }
+            [[maybe_unused]] typename M::R s_ps[9];
+            [[maybe_unused]] unsigned psbits = 0;
+            if constexpr (PS) {
+                psbits = g.ps[node];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) s_ps[k] = f[k];
+            }
             M::template collide<COLL>(f, rr, xr, yr, c);
 #pragma unroll
             for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
+            if constexpr (PS) {
+                if (psbits) ps_push(g, fout, node, psbits, s_ps, f, rr, xr, yr, c.ps_t);
+            }
         } else {
-            if (write_sector) {
+            // a partially saturated obstacle's slots hold what its neighbours write
+            if (write_sector && !(PS && cls == CLS_BB)) {
 #pragma unroll
                 for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
             }

@@ -1,0 +1,339 @@
+// Output writer (C ABI llb_writer_*): the reference's velocity text files
+// (util::writer::write_lattice_file<2>, utils/writers/LatticeWriter.hpp:60-92)
+// written off the stepping thread.
+//
+// A save enqueues a device-to-host copy of u into a pinned slot on the
+// lattice's own stream and records an event; the caller goes on enqueuing
+// steps.  One writer thread takes the slots in order, waits for each copy's
+// event, formats the rows on a few threads and writes the two files.  The
+// reference writes each value with `ostream << double` (default flags,
+// precision 6, i.e. printf "%.6g" in the C locale) followed by a space, and
+// ends each lattice row with std::endl; std::to_chars with
+// chars_format::general and precision 6 is specified as that same printf
+// conversion, so the bytes are identical.
+#include <algorithm>
+#include <cerrno>
+#include <charconv>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <system_error>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "llb_handle.h"
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Slot {
+    double* buf = nullptr;  // host memory, (R, C, 2) column-major
+    size_t cap = 0;         // doubles
+    bool pinned = false;    // page-locked (else malloc: host saves without a device)
+    cudaEvent_t ev = nullptr;
+    int ev_device = -1;
+    bool from_device = false;
+    int device = 0;
+    int64_t R = 0, C = 0, index = 0;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct llb_writer {
+    std::string dir;
+    int nthreads = 1;
+    std::vector<Slot> slots;
+    std::deque<int> queue;  // slots waiting for the writer thread, in save order
+    int writing = -1;       // slot the writer thread holds
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    std::thread io;
+    std::string bg_err;  // first error of the background work, not yet returned
+    int bg_rc = LLB_OK;
+    std::string err;     // message of the last failed call
+    int64_t files = 0;
+    double wait_s = 0.0, write_s = 0.0;
+    std::vector<std::string> bx, by;  // per formatting thread: rows of u_x, u_y
+};
+
+namespace {
+
+int wfail(llb_writer_handle w, int rc, const std::string& msg) {
+    if (w) w->err = msg;
+    return rc;
+}
+
+// Rows [i0, i1) of component files: value, space; newline after each row.
+void format_rows(const double* u, int64_t R, int64_t C, int64_t i0, int64_t i1, std::string& sx, std::string& sy) {
+    sx.clear();
+    sy.clear();
+    const int64_t N = R * C;
+    char tmp[64];
+    for (int64_t i = i0; i < i1; ++i) {
+        for (int d = 0; d < 2; ++d) {
+            std::string& s = d == 0 ? sx : sy;
+            const double* col = u + d * N + i;
+            for (int64_t j = 0; j < C; ++j) {
+                const auto r = std::to_chars(tmp, tmp + sizeof(tmp) - 1, col[j * R], std::chars_format::general, 6);
+                *r.ptr = ' ';
+                s.append(tmp, r.ptr + 1);
+            }
+            s.push_back('\n');
+        }
+    }
+}
+
+// Formats and writes one slot's two files; returns an error message or "".
+std::string write_slot(llb_writer* w, const Slot& s) {
+    const int64_t R = s.R, C = s.C;
+    const int T = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(w->nthreads, R)));
+    if (static_cast<int>(w->bx.size()) < T) {
+        w->bx.resize(T);
+        w->by.resize(T);
+    }
+    auto rows = [&](int t) { return std::make_pair(R * t / T, R * (t + 1) / T); };
+    std::vector<std::thread> pool;
+    pool.reserve(T - 1);
+    for (int t = 1; t < T; ++t)
+        pool.emplace_back([&, t] {
+            const auto [a, b] = rows(t);
+            format_rows(s.buf, R, C, a, b, w->bx[t], w->by[t]);
+        });
+    {
+        const auto [a, b] = rows(0);
+        format_rows(s.buf, R, C, a, b, w->bx[0], w->by[0]);
+    }
+    for (auto& th : pool) th.join();
+    for (int d = 0; d < 2; ++d) {
+        const std::string path = w->dir + "/output-" + std::to_string(s.index) + (d == 0 ? "u_x.txt" : "u_y.txt");
+        std::FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) return "cannot open " + path + ": " + std::strerror(errno);
+        bool ok = true;
+        for (int t = 0; t < T && ok; ++t) {
+            const std::string& b = d == 0 ? w->bx[t] : w->by[t];
+            ok = std::fwrite(b.data(), 1, b.size(), f) == b.size();
+        }
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) return "short write to " + path;
+    }
+    return "";
+}
+
+void io_loop(llb_writer* w) {
+    std::unique_lock<std::mutex> lk(w->mu);
+    for (;;) {
+        w->cv_work.wait(lk, [&] { return w->stop || !w->queue.empty(); });
+        if (w->queue.empty()) return;  // stop requested and nothing left
+        const int k = w->queue.front();
+        w->queue.pop_front();
+        w->writing = k;
+        Slot& s = w->slots[k];
+        lk.unlock();
+        std::string msg;
+        int rc = LLB_OK;
+        const double t0 = now_s();
+        if (s.from_device) {
+            cudaError_t e = cudaSetDevice(s.device);
+            if (e == cudaSuccess) e = cudaEventSynchronize(s.ev);
+            if (e != cudaSuccess) {
+                msg = std::string("copy of u: ") + cudaGetErrorString(e);
+                rc = LLB_E_CUDA;
+            }
+        }
+        const double t1 = now_s();
+        if (rc == LLB_OK) {
+            msg = write_slot(w, s);
+            if (!msg.empty()) rc = LLB_E_INVALID;
+        }
+        const double t2 = now_s();
+        lk.lock();
+        w->wait_s += t1 - t0;
+        w->write_s += t2 - t1;
+        if (rc == LLB_OK) ++w->files;
+        else if (w->bg_rc == LLB_OK) {
+            w->bg_rc = rc;
+            w->bg_err = msg;
+        }
+        s.busy = false;
+        w->writing = -1;
+        w->cv_done.notify_all();
+    }
+}
+
+// Takes the background error, if any, for the caller to return.
+int take_bg(llb_writer* w) {
+    if (w->bg_rc == LLB_OK) return LLB_OK;
+    const int rc = w->bg_rc;
+    w->err = w->bg_err;
+    w->bg_rc = LLB_OK;
+    w->bg_err.clear();
+    return rc;
+}
+
+void release_buf(Slot& s) {
+    if (s.buf) {
+        if (s.pinned) cudaFreeHost(s.buf);
+        else std::free(s.buf);
+    }
+    s.buf = nullptr;
+    s.cap = 0;
+    s.pinned = false;
+}
+
+// A free slot with room for n doubles, or -1 with w->err set.  Device saves
+// need page-locked memory for the copy to be asynchronous; host saves take
+// ordinary memory when no device is present.
+int acquire(llb_writer* w, std::unique_lock<std::mutex>& lk, size_t n, bool device, int& rc) {
+    int k = -1;
+    w->cv_done.wait(lk, [&] {
+        for (size_t i = 0; i < w->slots.size(); ++i)
+            if (!w->slots[i].busy) { k = static_cast<int>(i); return true; }
+        return false;
+    });
+    Slot& s = w->slots[k];
+    if (s.cap < n || (device && !s.pinned)) {
+        release_buf(s);
+        if (cudaHostAlloc(reinterpret_cast<void**>(&s.buf), n * sizeof(double), cudaHostAllocPortable) == cudaSuccess) {
+            s.pinned = true;
+        } else {
+            cudaGetLastError();
+            s.buf = device ? nullptr : static_cast<double*>(std::malloc(n * sizeof(double)));
+            if (!s.buf) {
+                rc = wfail(w, LLB_E_NOMEM, "host allocation of the output slot failed");
+                return -1;
+            }
+        }
+        s.cap = n;
+    }
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int llb_writer_create(const char* dir, int32_t slots, int32_t threads, llb_writer_handle* out) {
+    if (!dir || !out || slots < 0 || slots > 64 || threads < 0 || threads > 256) return LLB_E_INVALID;
+    *out = nullptr;
+    llb_writer* w = new (std::nothrow) llb_writer;
+    if (!w) return LLB_E_NOMEM;
+    w->dir = dir;
+    w->slots.resize(slots ? slots : 3);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    w->nthreads = threads ? threads : static_cast<int>(std::min(8u, hw));
+    w->io = std::thread(io_loop, w);
+    *out = w;
+    return LLB_OK;
+}
+
+int llb_writer_save_u(llb_writer_handle w, llb_handle h, int64_t index) {
+    if (!w || !h || index < 0) return wfail(w, LLB_E_INVALID, "bad arguments");
+    if (!h->macro_valid) return wfail(w, LLB_E_STATE, "no step has written u yet");
+    std::unique_lock<std::mutex> lk(w->mu);
+    int rc = take_bg(w);
+    if (rc) return rc;
+    const size_t n = static_cast<size_t>(h->R * h->C) * 2;
+    const int k = acquire(w, lk, n, true, rc);
+    if (k < 0) return rc;
+    Slot& s = w->slots[k];
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess && s.ev_device != h->device) {
+        if (s.ev) cudaEventDestroy(s.ev);
+        s.ev = nullptr;
+        s.ev_device = -1;
+        e = cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) s.ev_device = h->device;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.buf, h->d_u, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(s.ev, h->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return wfail(w, LLB_E_CUDA, std::string("enqueueing the copy of u: ") + cudaGetErrorString(e));
+    }
+    s.from_device = true;
+    s.device = h->device;
+    s.R = h->R;
+    s.C = h->C;
+    s.index = index;
+    s.busy = true;
+    w->queue.push_back(k);
+    w->cv_work.notify_one();
+    return LLB_OK;
+}
+
+int llb_writer_save_host(llb_writer_handle w, const double* u, int64_t rows, int64_t cols, int64_t index) {
+    if (!w || !u || rows < 1 || cols < 1 || rows > (1 << 30) || cols > (1 << 30) || rows * cols > (1LL << 36) ||
+        index < 0)
+        return wfail(w, LLB_E_INVALID, "bad arguments");
+    std::unique_lock<std::mutex> lk(w->mu);
+    int rc = take_bg(w);
+    if (rc) return rc;
+    const size_t n = static_cast<size_t>(rows * cols) * 2;
+    const int k = acquire(w, lk, n, false, rc);
+    if (k < 0) return rc;
+    Slot& s = w->slots[k];
+    std::memcpy(s.buf, u, n * sizeof(double));
+    s.from_device = false;
+    s.R = rows;
+    s.C = cols;
+    s.index = index;
+    s.busy = true;
+    w->queue.push_back(k);
+    w->cv_work.notify_one();
+    return LLB_OK;
+}
+
+int llb_writer_flush(llb_writer_handle w) {
+    if (!w) return LLB_E_INVALID;
+    std::unique_lock<std::mutex> lk(w->mu);
+    w->cv_done.wait(lk, [&] {
+        return std::none_of(w->slots.begin(), w->slots.end(), [](const Slot& s) { return s.busy; });
+    });
+    return take_bg(w);
+}
+
+int llb_writer_stats(llb_writer_handle w, int64_t* files, double* wait_s, double* write_s) {
+    if (!w) return LLB_E_INVALID;
+    std::lock_guard<std::mutex> lk(w->mu);
+    if (files) *files = w->files;
+    if (wait_s) *wait_s = w->wait_s;
+    if (write_s) *write_s = w->write_s;
+    return LLB_OK;
+}
+
+int llb_writer_destroy(llb_writer_handle w) {
+    if (!w) return LLB_OK;
+    const int rc = llb_writer_flush(w);
+    {
+        std::lock_guard<std::mutex> lk(w->mu);
+        w->stop = true;
+    }
+    w->cv_work.notify_all();
+    if (w->io.joinable()) w->io.join();
+    for (Slot& s : w->slots) {
+        release_buf(s);
+        if (s.ev) {
+            cudaSetDevice(s.ev_device);
+            cudaEventDestroy(s.ev);
+        }
+    }
+    delete w;
+    return rc;
+}
+
+const char* llb_writer_last_error(llb_writer_handle w) { return w ? w->err.c_str() : "null writer"; }
+
+}  // extern "C"

@@ -12,7 +12,8 @@
  *
  * The Configuration keeps the reference's policy types (any of the Serial,
  * OpenMP, std::execution and OpenACC families): BGK or TRT collision,
- * BounceBack walls and obstacles, ZouHe / OpenBoundary / ZouHePressure
+ * BounceBack walls and obstacles (obstacles also PSBounceBack, partially
+ * saturated), ZouHe / OpenBoundary / ZouHePressure
  * inlets and outlets, VelocityInitializer, DefaultEquilibrium.  Their static
  * parameters (tau, tau_even / tau_odd, the update functions, the pressure
  * policy's rho_out) are read when perform_lbm starts, as the reference's
@@ -34,6 +35,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <iostream>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -61,6 +63,12 @@ namespace llalbm::core
         template <class B>
         inline constexpr bool is_bounce_back = is_any<B, boundaries::BounceBackPolicy, boundaries::OMPBounceBackPolicy,
                                                       boundaries::STDExecBounceBackPolicy, boundaries::OpenACCBounceBackPolicy>;
+        // partially saturated bounce-back (PSBounceBackPolicy.hpp): plain
+        // bounce-back on walls, the partially saturated rule on obstacles
+        template <class B>
+        inline constexpr bool is_ps_bounce_back =
+            is_any<B, boundaries::PSBounceBackPolicy, boundaries::OMPPSBounceBackPolicy,
+                   boundaries::STDExecPSBounceBackPolicy, boundaries::OpenACCPSBounceBackPolicy>;
         template <class B>
         inline constexpr bool is_zou_he = is_any<B, boundaries::ZouHePolicy, boundaries::OMPZouHePolicy,
                                                  boundaries::STDExecZouHePolicy, boundaries::OpenACCZouHePolicy>;
@@ -101,6 +109,21 @@ namespace llalbm::core
             }
         };
         using Handle = std::unique_ptr<llb_lattice, HandleDeleter>;
+
+        struct WriterDeleter
+        {
+            void operator()(llb_writer* w) const
+            {
+                if (w) llb_writer_destroy(w);
+            }
+        };
+        using Writer = std::unique_ptr<llb_writer, WriterDeleter>;
+
+        inline void check_writer(int rc, llb_writer_handle w, const char* what)
+        {
+            if (rc != LLB_OK)
+                throw std::runtime_error(std::string("CUDAPolicy: ") + what + ": " + llb_writer_last_error(w));
+        }
     }  // namespace cuda_detail
 
     template <std::size_t dim, typename Configuration>
@@ -126,8 +149,10 @@ namespace llalbm::core
         static_assert(dims == 2, "CUDAPolicy implements the D2Q9 lattice only");
         static_assert(cuda_detail::is_bgk<CollisionPolicy> || cuda_detail::is_trt<CollisionPolicy>,
                       "CUDAPolicy: the collision policy must be a BGK or TRT policy");
-        static_assert(cuda_detail::is_bounce_back<WallPolicy> && cuda_detail::is_bounce_back<ObstaclePolicy>,
-                      "CUDAPolicy: walls and obstacles must use a BounceBack policy");
+        static_assert((cuda_detail::is_bounce_back<WallPolicy> || cuda_detail::is_ps_bounce_back<WallPolicy>) &&
+                          (cuda_detail::is_bounce_back<ObstaclePolicy> ||
+                           cuda_detail::is_ps_bounce_back<ObstaclePolicy>),
+                      "CUDAPolicy: walls and obstacles must use a BounceBack or PSBounceBack policy");
         static_assert(cuda_detail::open_bc<InletPolicy>() >= 0 && cuda_detail::open_bc<OutletPolicy>() >= 0,
                       "CUDAPolicy: inlets/outlets must use ZouHe, OpenBoundary or ZouHePressure");
         static_assert(cuda_detail::is_velocity_init<InitializationPolicy>,
@@ -284,6 +309,16 @@ namespace llalbm::core
             d.inlet_bc = Policy::inlet_bc;
             d.outlet_bc = Policy::outlet_bc;
             Policy::fill_collision(d);
+            std::vector<double> obstacle_b;
+            if constexpr (cuda_detail::is_ps_bounce_back<typename Policy::ObstaclePolicy>)
+            {
+                // the policy's tau and each obstacle's b, read when the run starts
+                d.obstacle_bc = LLB_OBSTACLE_PARTIAL;
+                d.ps_tau = Policy::ObstaclePolicy::tau;
+                obstacle_b.resize(obstacle_nodes.size());
+                for (std::size_t n = 0; n < obstacle_nodes.size(); ++n) obstacle_b[n] = obstacle_nodes[n].get_b();
+                d.obstacle_b = obstacle_b.data();
+            }
             d.storage = LLB_STORE_F64;
             d.pattern = LLB_PATTERN_AB;
             d.device = device;
@@ -384,6 +419,11 @@ namespace llalbm::core
          * fresh equilibrium start, `time / time_step` steps, u written to
          * results/ every save_step steps, FlowAnalyzer hook, NaN check under
          * LLALBM_DEBUG.  The update functions receive the step index as time.
+         * The output files are the reference writer's, byte for byte
+         * (LatticeWriter.hpp:60-92); a save only enqueues the copy of u on the
+         * engine's stream, and a native writer thread formats and writes the
+         * files while the next steps run.  All files are written when
+         * perform_lbm returns.
          */
         void perform_lbm(const double time, const double time_step = 1, const std::size_t save_step = 1,
                          const bool should_save = true)
@@ -398,6 +438,18 @@ namespace llalbm::core
             const std::size_t n_steps = static_cast<std::size_t>(time / time_step);
             create_engine();
             llb_handle h = engine.get();
+            cuda_detail::Writer writer;
+            if (should_save)
+            {
+                llb_writer_handle w = nullptr;
+                const int rc = llb_writer_create(llalbm::util::writer::output_dir_path.c_str(), 3, 0, &w);
+                if (rc != LLB_OK) throw std::runtime_error("CUDAPolicy: llb_writer_create failed");
+                writer.reset(w);
+            }
+            auto save = [&](std::size_t n) {
+                cuda_detail::check_writer(llb_writer_save_u(writer.get(), h, static_cast<int64_t>(n)), writer.get(),
+                                          "llb_writer_save_u");
+            };
             std::vector<ObstaclePoint<2>> analyzer_points;
             if (flow_analyzer)
             {
@@ -424,11 +476,7 @@ namespace llalbm::core
             upload_values(0, std::min<std::size_t>(CHUNK, std::max<std::size_t>(n_steps, 1)), buf);
             const bool macro0 = is_save(0) || n_steps == 1;
             cuda_detail::check(llb_init(h, macro0 ? LLB_STEP_MACRO : 0u), h, "llb_init");
-            if (is_save(0))
-            {
-                pull_macro();
-                llalbm::util::writer::write_lattice_file<2>(global_u, saved_file++);
-            }
+            if (is_save(0)) save(saved_file++);
             std::size_t uploaded_to = std::min<std::size_t>(CHUNK, n_steps);  // rows [0, uploaded_to) are set
             std::size_t i = 1;
             while (i < n_steps)
@@ -452,11 +500,7 @@ namespace llalbm::core
 #ifndef LLALBM_VERBOSE
                 std::cout << "\rStep " + std::to_string(last) + " / " + std::to_string(n_steps) << std::flush;
 #endif
-                if (is_save(last))
-                {
-                    pull_macro();
-                    llalbm::util::writer::write_lattice_file<2>(global_u, saved_file++);
-                }
+                if (is_save(last)) save(saved_file++);
                 if (is_analysis(last)) analyze(analyzer_points);
 #ifdef LLALBM_DEBUG
                 if (llb_check_numerics(h) == LLB_E_NUMERIC)
@@ -468,6 +512,8 @@ namespace llalbm::core
                 i = last + 1;
             }
             cuda_detail::check(llb_synchronize(h), h, "llb_synchronize");
+            if (writer)
+                cuda_detail::check_writer(llb_writer_flush(writer.get()), writer.get(), "llb_writer_flush");
             pull_macro();  // global_rho / global_u of the last step, as the reference leaves them
 #ifdef TIMER
             const auto end = std::chrono::high_resolution_clock::now();
@@ -533,6 +579,23 @@ namespace llalbm::core
         void attach_flow_analyzer(std::shared_ptr<llalbm::analysis::FlowAnalyzer<2>> flow_analyzer_)
         {
             flow_analyzer = flow_analyzer_->shared_from_this();
+        }
+
+        /**
+         * The reference's weight pass for partially saturated obstacles
+         * (Lattice.hpp:245-278): b of every obstacle in a 5 x 5 block = the
+         * block's obstacle count / 25.  The reference stores those weights
+         * into copies of the nodes it groups by block, so the lattice's own
+         * obstacle nodes keep their b (1 unless set before reinit); the same
+         * happens here, which keeps the runs identical to the reference's.
+         */
+        void compute_obstacle_weight()
+        {
+            std::map<std::pair<int, int>, std::vector<ObstaclePoint<2>>> blocks;
+            for (const auto& p : obstacle_nodes)
+                blocks[{static_cast<int>(p.coords[0] / 5), static_cast<int>(p.coords[1] / 5)}].push_back(p);
+            for (auto& block : blocks)
+                for (auto& p : block.second) p.set_b(static_cast<double>(block.second.size()) / 25.0);
         }
     };
 }  // namespace llalbm::core

@@ -28,6 +28,7 @@ BGK, TRT = 0, 1
 STORE_F64, STORE_F32S, STORE_F16S = 0, 1, 2
 PATTERN_AB, PATTERN_AA = 0, 1
 BC_ZH_VELOCITY, BC_OPEN, BC_ZH_PRESSURE = 0, 1, 2
+OBSTACLE_BOUNCE_BACK, OBSTACLE_PARTIAL = 0, 1
 STEP_MACRO = 1
 SERVE_BATCHED, SERVE_SEQUENTIAL = 0, 1
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
@@ -53,6 +54,7 @@ class _Desc(ctypes.Structure):
         ("tau_even", ctypes.c_double), ("tau_odd", ctypes.c_double),
         ("storage", ctypes.c_int32), ("pattern", ctypes.c_int32),
         ("device", ctypes.c_int32), ("open_table_rows", ctypes.c_int32),
+        ("obstacle_bc", ctypes.c_int32), ("ps_tau", ctypes.c_double), ("obstacle_b", ctypes.c_void_p),
     ]
 
 
@@ -131,6 +133,14 @@ SIGNATURES = {
     "llb_server_result": [_H, ctypes.c_int64, _P, _P, _P],
     "llb_server_stats": [_H, _P],
     "llb_server_last_error": [_H],
+    "llb_writer_create": [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_H)],
+    "llb_writer_save_u": [_H, _H, ctypes.c_int64],
+    "llb_writer_save_host": [_H, _P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64],
+    "llb_writer_flush": [_H],
+    "llb_writer_stats": [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_double)],
+    "llb_writer_destroy": [_H],
+    "llb_writer_last_error": [_H],
 }
 
 
@@ -185,7 +195,8 @@ def classify(types: np.ndarray) -> dict:
 
 
 def _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs, *,
-          collision, tau, tau_even, tau_odd, inlet_bc, outlet_bc, storage, pattern, device, open_table_rows):
+          collision, tau, tau_even, tau_odd, inlet_bc, outlet_bc, storage, pattern, device, open_table_rows,
+          obstacle_bc=OBSTACLE_BOUNCE_BACK, ps_tau=0.6, obstacle_b=None):
     """Descriptor plus the arrays it points into (keep them alive while it is used)."""
     keep = {
         "fluid": _ij(fluid), "wall": _ij(wall), "inlet": _ij(inlet), "outlet": _ij(outlet),
@@ -200,7 +211,11 @@ def _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obsta
               len(keep["inlet"]), _ptr(keep["inlet"]), _ptr(keep["inlet_side"]),
               len(keep["outlet"]), _ptr(keep["outlet"]), _ptr(keep["outlet_side"]),
               len(keep["obstacle"]), _ptr(keep["obstacle"]), _ptr(keep["obstacle_dirs"]),
-              inlet_bc, outlet_bc, collision, tau, tau_even, tau_odd, storage, pattern, device, open_table_rows)
+              inlet_bc, outlet_bc, collision, tau, tau_even, tau_odd, storage, pattern, device, open_table_rows,
+              obstacle_bc, ps_tau, None)
+    if obstacle_b is not None:
+        keep["obstacle_b"] = np.ascontiguousarray(np.asarray(obstacle_b, dtype=np.float64).reshape(-1))
+        d.obstacle_b = _ptr(keep["obstacle_b"])
     return d, keep
 
 
@@ -221,14 +236,16 @@ class CudaLattice:
                  obstacle, obstacle_dirs=None, *, collision: int = BGK, tau: float = 0.6,
                  tau_even: float = 0.6, tau_odd: float = 0.6, inlet_bc: int = BC_ZH_VELOCITY,
                  outlet_bc: int = BC_ZH_VELOCITY, storage: int = STORE_F64, pattern: int = PATTERN_AB,
-                 device: int = 0, open_table_rows: int = 1):
+                 device: int = 0, open_table_rows: int = 1, obstacle_bc: int = OBSTACLE_BOUNCE_BACK,
+                 ps_tau: float = 0.6, obstacle_b=None):
         self.rows, self.cols = int(rows), int(cols)
         self.storage = storage
         self._owner = True
         d, keep = _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs,
                         collision=collision, tau=tau, tau_even=tau_even, tau_odd=tau_odd, inlet_bc=inlet_bc,
                         outlet_bc=outlet_bc, storage=storage, pattern=pattern, device=device,
-                        open_table_rows=open_table_rows)
+                        open_table_rows=open_table_rows, obstacle_bc=obstacle_bc, ps_tau=ps_tau,
+                        obstacle_b=obstacle_b)
         self.n_inlet, self.n_outlet = len(keep["inlet"]), len(keep["outlet"])
         self.n_open = self.n_inlet + self.n_outlet
         self.n_active = len(keep["fluid"]) + self.n_open
@@ -403,13 +420,14 @@ class CudaBatch:
 
     def add(self, rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs=None, *,
             collision=BGK, tau=0.6, tau_even=0.6, tau_odd=0.6, inlet_bc=BC_ZH_VELOCITY, outlet_bc=BC_ZH_VELOCITY,
-            open_values=None) -> int:
+            open_values=None, obstacle_bc=OBSTACLE_BOUNCE_BACK, ps_tau=0.6, obstacle_b=None) -> int:
         vals = None if open_values is None else np.ascontiguousarray(open_values, dtype=np.float64)
         nrows = 0 if vals is None else vals.reshape(-1, len(inlet) + len(outlet), 2).shape[0]
         d, keep = _desc(rows, cols, fluid, wall, inlet, inlet_side, outlet, outlet_side, obstacle, obstacle_dirs,
                         collision=collision, tau=tau, tau_even=tau_even, tau_odd=tau_odd, inlet_bc=inlet_bc,
                         outlet_bc=outlet_bc, storage=self.storage, pattern=PATTERN_AB, device=self.device,
-                        open_table_rows=max(nrows, 1))
+                        open_table_rows=max(nrows, 1), obstacle_bc=obstacle_bc, ps_tau=ps_tau,
+                        obstacle_b=obstacle_b)
         slot = ctypes.c_int32()
         _bcheck(lib().llb_batch_add(self._b, ctypes.byref(d), _ptr(vals), nrows, ctypes.byref(slot)), self._b)
         n_in, n_out = len(keep["inlet"]), len(keep["outlet"])
@@ -564,3 +582,54 @@ class CudaServer:
         c = _ServerCounters()
         _scheck(lib().llb_server_stats(self._s, ctypes.byref(c)), self._s)
         return {k: getattr(c, k) for k, _ in c._fields_}
+
+
+def _wcheck(rc: int, w):
+    if rc != LLB_OK:
+        msg = lib().llb_writer_last_error(w) if w else b""
+        raise LLBError(rc, msg.decode() if msg else "")
+
+
+class OutputWriter:
+    """The reference's velocity output files (LatticeWriter.hpp:60-92:
+    <dir>/output-<n>u_x.txt, u_y.txt) written by a native thread while the
+    caller keeps stepping.  save_u(lattice, n) enqueues the copy of the last
+    macro step's u on the lattice's stream and returns; flush() waits for every
+    queued file."""
+
+    def __init__(self, directory: str, slots: int = 3, threads: int = 0):
+        h = _H()
+        rc = lib().llb_writer_create(str(directory).encode(), slots, threads, ctypes.byref(h))
+        if rc != LLB_OK:
+            raise LLBError(rc, "llb_writer_create")
+        self._w = h
+
+    def save_u(self, lattice: "CudaLattice", index: int):
+        _wcheck(lib().llb_writer_save_u(self._w, lattice._h, index), self._w)
+
+    def save_host(self, u: np.ndarray, index: int):
+        """u: an (R, C, 2) array, u[i, j, d] as the reference's global_u(i, j, d)."""
+        R, C = int(u.shape[0]), int(u.shape[1])
+        flat = np.ascontiguousarray(np.ravel(np.asarray(u, dtype=np.float64), order="F"))
+        _wcheck(lib().llb_writer_save_host(self._w, _ptr(flat), R, C, index), self._w)
+
+    def flush(self):
+        _wcheck(lib().llb_writer_flush(self._w), self._w)
+
+    def stats(self) -> dict:
+        n, a, b = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        _wcheck(lib().llb_writer_stats(self._w, ctypes.byref(n), ctypes.byref(a), ctypes.byref(b)), self._w)
+        return {"files": n.value, "wait_s": a.value, "write_s": b.value}
+
+    def close(self):
+        if self._w:
+            w, self._w = self._w, None
+            rc = lib().llb_writer_destroy(w)
+            if rc != LLB_OK:
+                raise LLBError(rc, "llb_writer_destroy")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -158,6 +158,80 @@ static void bounce_obstacles(lattice_t* L, const int64_t* nodes, const uint16_t*
     }
 }
 
+/* PSBounceBackPolicy<2>::update_boundaries on obstacle nodes
+   (PSBounceBackPolicy.hpp:177-293): for each set bit k the fluid neighbour
+   x + c_k receives a mix of the relaxed reflection and its own previous value,
+   with e from the neighbour's global_rho/global_u and the obstacle's global_rho
+   (1, never updated for obstacles). */
+static void ps_obstacles(lattice_t* L, const int64_t* nodes, const uint16_t* dirs, const double* bvals, int64_t n,
+                         double tau)
+{
+    const double two9 = (2.0 / 9.0);
+    const double one18 = (1.0 / 18.0);
+    const double one36 = (1.0 / 36.0);
+    (void)two9;
+    for (int64_t q = 0; q < n; ++q) {
+        const int64_t i = nodes[2 * q], j = nodes[2 * q + 1];
+        const double b = bvals ? bvals[q] : 1.0;
+        const double p1 = P(L->pop, i, j, 1), p2 = P(L->pop, i, j, 2), p3 = P(L->pop, i, j, 3);
+        const double p4 = P(L->pop, i, j, 4), p5 = P(L->pop, i, j, 5), p6 = P(L->pop, i, j, 6);
+        const double p7 = P(L->pop, i, j, 7), p8 = P(L->pop, i, j, 8);
+        const double t = 1.0 / tau;
+        const double rx = RHO(i, j);
+        double rho, ux, uy, u2, ea, eb;
+#define MAC(ii, jj) rho = RHO(ii, jj); ux = U(ii, jj, 0); uy = U(ii, jj, 1); u2 = ux * ux + uy * uy
+        if (dirs[q] & (1u << 1)) {
+            MAC(i, j + 1);
+            ea = one18 * rho * (2 + 6 * ux + 9 * ux * ux - 3 * u2);  /* e1 */
+            eb = one18 * rho * (2 - 6 * ux + 9 * ux * ux - 3 * u2);  /* e3 */
+            P(L->pop, i, j + 1, 1) = p3 - (1.0 - b) * (p3 - eb) * t + b * ((P(L->pop, i, j + 1, 1) - ea) - (p3 - 2 * one18 * rx));
+        }
+        if (dirs[q] & (1u << 2)) {
+            MAC(i - 1, j);
+            ea = one18 * rho * (2 + 6 * uy + 9 * uy * uy - 3 * u2);  /* e2 */
+            eb = one18 * rho * (2 - 6 * uy + 9 * uy * uy - 3 * u2);  /* e4 */
+            P(L->pop, i - 1, j, 2) = p4 - (1.0 - b) * (p4 - eb) * t + b * ((P(L->pop, i - 1, j, 2) - ea) - (p4 - 2 * one18 * rx));
+        }
+        if (dirs[q] & (1u << 3)) {
+            MAC(i, j - 1);
+            ea = one18 * rho * (2 + 6 * ux + 9 * ux * ux - 3 * u2);  /* e1 */
+            eb = one18 * rho * (2 - 6 * ux + 9 * ux * ux - 3 * u2);  /* e3 */
+            P(L->pop, i, j - 1, 3) = p1 - (1.0 - b) * (p1 - ea) * t + b * ((P(L->pop, i, j - 1, 3) - eb) - (p1 - 2 * one18 * rx));
+        }
+        if (dirs[q] & (1u << 4)) {
+            MAC(i + 1, j);
+            ea = one18 * rho * (2 + 6 * uy + 9 * uy * uy - 3 * u2);  /* e2 */
+            eb = one18 * rho * (2 - 6 * uy + 9 * uy * uy - 3 * u2);  /* e4 */
+            P(L->pop, i + 1, j, 4) = p2 - (1.0 - b) * (p2 - ea) * t + b * ((P(L->pop, i + 1, j, 4) - eb) - (p2 - 2 * one18 * rx));
+        }
+        if (dirs[q] & (1u << 5)) {
+            MAC(i - 1, j + 1);
+            ea = one36 * rho * (1 + 3 * (ux + uy) + 9 * ux * uy + 3 * u2);  /* e5 */
+            eb = one36 * rho * (1 - 3 * (ux + uy) + 9 * ux * uy + 3 * u2);  /* e7 */
+            P(L->pop, i - 1, j + 1, 5) = p7 - (1.0 - b) * (p7 - eb) * t + b * ((P(L->pop, i - 1, j + 1, 5) - ea) - (p7 - one36 * rx));
+        }
+        if (dirs[q] & (1u << 6)) {
+            MAC(i - 1, j - 1);
+            ea = one36 * rho * (1 - 3 * (ux - uy) - 9 * ux * uy + 3 * u2);  /* e6 */
+            eb = one36 * rho * (1 + 3 * (ux - uy) - 9 * ux * uy + 3 * u2);  /* e8 */
+            P(L->pop, i - 1, j - 1, 6) = p8 - (1.0 - b) * (p8 - eb) * t + b * ((P(L->pop, i - 1, j - 1, 6) - ea) - (p8 - one36 * rx));
+        }
+        if (dirs[q] & (1u << 7)) {
+            MAC(i + 1, j - 1);
+            ea = one36 * rho * (1 + 3 * (ux + uy) + 9 * ux * uy + 3 * u2);  /* e5 */
+            eb = one36 * rho * (1 - 3 * (ux + uy) + 9 * ux * uy + 3 * u2);  /* e7 */
+            P(L->pop, i + 1, j - 1, 7) = p5 - (1.0 - b) * (p5 - ea) * t + b * ((P(L->pop, i + 1, j - 1, 7) - eb) - (p5 - one36 * rx));
+        }
+        if (dirs[q] & (1u << 8)) {
+            MAC(i + 1, j + 1);
+            ea = one36 * rho * (1 - 3 * (ux - uy) - 9 * ux * uy + 3 * u2);  /* e6 */
+            eb = one36 * rho * (1 + 3 * (ux - uy) - 9 * ux * uy + 3 * u2);  /* e8 */
+            P(L->pop, i + 1, j + 1, 8) = p6 - (1.0 - b) * (p6 - ea) * t + b * ((P(L->pop, i + 1, j + 1, 8) - eb) - (p6 - one36 * rx));
+        }
+#undef MAC
+    }
+}
+
 /* ZouHePolicy<2>::update_boundaries (ZouHePolicy.hpp:58-123).  global_u is the
    by-value copy the policy receives; the density it computes is stored into a
    copy and lost, so it is not kept here. */
@@ -408,7 +482,10 @@ int lbo_run(const lbo_problem* pr, int64_t steps, const double* open_u, int64_t 
         stream_open(L, pr->inlet, pr->n_inlet);
         stream_open(L, pr->outlet, pr->n_outlet);
         bounce_walls(L, pr->wall, pr->n_wall);                                                     /* :402 */
-        bounce_obstacles(L, pr->obst, pr->obst_dirs, pr->n_obst);                                  /* :403 */
+        if (pr->obstacle_bc == LBO_OBST_PARTIAL)                                                   /* :403 */
+            ps_obstacles(L, pr->obst, pr->obst_dirs, pr->obst_b, pr->n_obst, pr->ps_tau);
+        else
+            bounce_obstacles(L, pr->obst, pr->obst_dirs, pr->n_obst);
         if (pr->inlet_bc == LBO_BC_ZH_VELOCITY)                                                    /* :409 */
             zou_he_velocity(L, pr->inlet, pr->inlet_side, pr->n_inlet);
         else if (pr->inlet_bc == LBO_BC_ZH_PRESSURE)

@@ -24,6 +24,8 @@ enum { LBO_BGK = 0, LBO_TRT = 1 };
 /* open-boundary policies: Zou-He velocity (ZouHePolicy), open no-op
    (OpenBoundaryPolicy), Zou-He pressure (the extension in ZouHePressurePolicy.hpp) */
 enum { LBO_BC_ZH_VELOCITY = 0, LBO_BC_OPEN = 1, LBO_BC_ZH_PRESSURE = 2 };
+/* obstacle policies: BounceBackPolicy, PSBounceBackPolicy (partially saturated) */
+enum { LBO_OBST_BOUNCE_BACK = 0, LBO_OBST_PARTIAL = 1 };
 
 typedef struct {
     int64_t rows, cols;
@@ -36,6 +38,9 @@ typedef struct {
     double tau, tau_even, tau_odd;
     int32_t inlet_bc, outlet_bc;       /* LBO_BC_* */
     double rho_out, tangential_u;      /* Zou-He pressure parameters */
+    int32_t obstacle_bc;               /* LBO_OBST_* */
+    double ps_tau;                     /* PSBounceBackPolicy<2>::tau */
+    const double* obst_b;              /* per obstacle b (ObstaclePoint::get_b), NULL: 1.0 */
 } lbo_problem;
 
 /*

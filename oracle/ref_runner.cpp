@@ -41,6 +41,8 @@ struct Options {
     std::string inlet_u = "const:0:0";
     std::string outlet_u = "const:0:0";
     double rho_out = 1.0, tangential_u = 0.0;
+    std::string obstacle = "bb";    // bb | ps (PSBounceBackPolicy, serial policies)
+    double ps_tau = 0.6;
     long steps = 10;
     long warmup = 0;
     long analyzer_every = 0;
@@ -290,7 +292,7 @@ void set_collision(const Options& o) {
 template <bool OMP, typename C> struct ParOf { using type = SerialPolicy<2, C>; };
 template <typename C> struct ParOf<true, C> { using type = OMPPolicy<2, C>; };
 
-template <bool OMP, bool TRT, int IN, int OUT>
+template <bool OMP, bool TRT, int IN, int OUT, bool PS = false>
 struct Select {
     template <typename S, typename M> using pick = std::conditional_t<OMP, M, S>;
     using Coll = std::conditional_t<TRT, pick<collisions::TRTCollisionPolicy<2>, collisions::OMPTRTCollisionPolicy<2>>,
@@ -303,13 +305,14 @@ struct Select {
     using Out = std::conditional_t<OUT == 0, ZH, std::conditional_t<OUT == 1, Open, ZHP>>;
     using Init = pick<initializers::VelocityInitializer<2>, initializers::OMPVelocityInitializer<2>>;
     using Eq = pick<equilibrium::DefaultEquilibrium<2>, equilibrium::OMPDefaultEquilibrium<2>>;
-    using Config = LatticeConfiguration<2, Coll, BB, BB, In, Out, Init, Eq>;
+    using Obst = std::conditional_t<PS, pick<boundaries::PSBounceBackPolicy<2>, boundaries::OMPPSBounceBackPolicy<2>>, BB>;
+    using Config = LatticeConfiguration<2, Coll, BB, Obst, In, Out, Init, Eq>;
     using Par = typename ParOf<OMP, Config>::type;
 };
 
-template <bool OMP, bool TRT, int IN, int OUT>
+template <bool OMP, bool TRT, int IN, int OUT, bool PS = false>
 int run_case(const Options& o) {
-    using S = Select<OMP, TRT, IN, OUT>;
+    using S = Select<OMP, TRT, IN, OUT, PS>;
     using Par = typename S::Par;
     std::ofstream log(o.out + "/ref_runner.log");
     std::unique_ptr<Lattice<Par>> lat;
@@ -324,6 +327,12 @@ int run_case(const Options& o) {
     if (o.dump_nodes) dump_nodes(*lat, o.out);
 
     set_collision<typename S::Coll>(o);
+    if constexpr (PS) {
+        // the reference's own set-up sequence (test/unit/LidWithPSObstacle.cpp:74-76);
+        // compute_obstacle_weight fills copies of the nodes, so every b stays 1
+        S::Obst::initialize(o.ps_tau);
+        lat->compute_obstacle_weight();
+    }
     boundaries::ZouHePressurePolicy<2>::initialize(o.rho_out, o.tangential_u);
     boundaries::ZouHePressurePolicy<2>::reset();
     auto inlets = make_functions(o.inlet_u);
@@ -372,6 +381,14 @@ int dispatch_bc(const Options& o) {
     const int in = o.inlet_bc == "zh" ? 0 : o.inlet_bc == "open" ? 1 : -1;
     const int out = o.outlet_bc == "zh" ? 0 : o.outlet_bc == "open" ? 1 : o.outlet_bc == "zhp" ? 2 : -1;
     if (in < 0 || out < 0) die("bad boundary policy");
+    if (o.obstacle == "ps") {
+        // partially saturated obstacles: Zou-He velocity inlets only
+        if (in != 0) die("ps obstacles run with zh inlets");
+        if (out == 0) return run_case<OMP, TRT, 0, 0, true>(o);
+        if (out == 1) return run_case<OMP, TRT, 0, 1, true>(o);
+        return run_case<OMP, TRT, 0, 2, true>(o);
+    }
+    if (o.obstacle != "bb") die("bad obstacle policy");
     if (in == 0 && out == 0) return run_case<OMP, TRT, 0, 0>(o);
     if (in == 0 && out == 1) return run_case<OMP, TRT, 0, 1>(o);
     if (in == 0 && out == 2) return run_case<OMP, TRT, 0, 2>(o);
@@ -405,6 +422,8 @@ int main(int argc, char** argv) {
         else if (k == "--outlet-u") o.outlet_u = val();
         else if (k == "--rho-out") o.rho_out = std::stod(val());
         else if (k == "--tangential-u") o.tangential_u = std::stod(val());
+        else if (k == "--obstacle") o.obstacle = val();
+        else if (k == "--ps-tau") o.ps_tau = std::stod(val());
         else if (k == "--steps") o.steps = std::stol(val());
         else if (k == "--warmup") o.warmup = std::stol(val());
         else if (k == "--analyzer") o.analyzer_every = std::stol(val());
@@ -420,6 +439,7 @@ int main(int argc, char** argv) {
     const bool trt = o.collision == "trt";
     if (o.policy != "omp" && o.policy != "serial") die("bad policy");
     if (o.collision != "trt" && o.collision != "bgk") die("bad collision");
+    if (omp && o.obstacle == "ps") die("ps obstacles run with the serial policies");
     if (omp && trt) return dispatch_bc<true, true>(o);
     if (omp) return dispatch_bc<true, false>(o);
     if (trt) return dispatch_bc<false, true>(o);

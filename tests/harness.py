@@ -146,6 +146,7 @@ class _Problem(ctypes.Structure):
         ("collision", ctypes.c_int32), ("tau", ctypes.c_double), ("tau_even", ctypes.c_double),
         ("tau_odd", ctypes.c_double), ("inlet_bc", ctypes.c_int32), ("outlet_bc", ctypes.c_int32),
         ("rho_out", ctypes.c_double), ("tangential_u", ctypes.c_double),
+        ("obstacle_bc", ctypes.c_int32), ("ps_tau", ctypes.c_double), ("obst_b", ctypes.c_void_p),
     ]
 
 
@@ -177,6 +178,9 @@ class Params:
     outlet_bc: int = BC_ZH_VELOCITY
     rho_out: float = 1.0
     tangential_u: float = 0.0
+    obstacle_bc: int = 0          # 0 bounce-back, 1 partially saturated (PSBounceBackPolicy)
+    ps_tau: float = 0.6
+    obstacle_b: object = None     # per obstacle b (ObstaclePoint::get_b), None: 1.0
 
     @staticmethod
     def trt_magic(tau_even: float, magic: float = 0.25, **kw) -> "Params":
@@ -197,13 +201,16 @@ def run_oracle(lists: NodeLists, params: Params, steps: int, table: np.ndarray,
         "obst": np.ascontiguousarray(lists.obstacle, dtype=np.int64),
         "obst_dirs": np.ascontiguousarray(lists.obstacle_dirs, dtype=np.uint16),
     }
+    if params.obstacle_b is not None:
+        arrs["obst_b"] = np.ascontiguousarray(params.obstacle_b, dtype=np.float64)
     pr = _Problem(lists.rows, lists.cols,
                   len(arrs["fluid"]), _ptr(arrs["fluid"]), len(arrs["wall"]), _ptr(arrs["wall"]),
                   len(arrs["inlet"]), _ptr(arrs["inlet"]), _ptr(arrs["inlet_side"]),
                   len(arrs["outlet"]), _ptr(arrs["outlet"]), _ptr(arrs["outlet_side"]),
                   len(arrs["obst"]), _ptr(arrs["obst"]), _ptr(arrs["obst_dirs"]),
                   params.collision, params.tau, params.tau_even, params.tau_odd,
-                  params.inlet_bc, params.outlet_bc, params.rho_out, params.tangential_u)
+                  params.inlet_bc, params.outlet_bc, params.rho_out, params.tangential_u,
+                  params.obstacle_bc, params.ps_tau, _ptr(arrs["obst_b"]) if "obst_b" in arrs else None)
     R, C = lists.rows, lists.cols
     pop = np.zeros((9, C, R)); u = np.zeros((2, C, R)); rho = np.zeros((C, R)); post = np.zeros((9, C, R))
     table = np.ascontiguousarray(table, dtype=np.float64)

@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol(cuda_lib):
     for n in names:
         assert hasattr(cuda_lib, n), n
         assert n in L.SIGNATURES, n
-    assert cuda_lib.llb_abi_version() == 1
+    assert cuda_lib.llb_abi_version() == 2
 
 
 @pytest.mark.parametrize("types", [
@@ -102,6 +102,14 @@ def test_create_validates_before_touching_a_device():
     with pytest.raises(L.LLBError) as e:
         L.CudaLattice(**kw)
     assert e.value.code == -2
+    # a bad obstacle policy, and partially saturated b outside [0, 1]
+    with pytest.raises(L.LLBError) as e:
+        L.CudaLattice(**_desc_kw(lists), obstacle_bc=7)
+    assert e.value.code == -1
+    with pytest.raises(L.LLBError) as e:
+        L.CudaLattice(**_desc_kw(lists), obstacle_bc=1, ps_tau=0.6,
+                      obstacle_b=np.full(len(lists.obstacle), 1.5))
+    assert e.value.code == -1
     # obstacle bits that are not the reference's neighbour rule
     kw = _desc_kw(lists)
     kw["obstacle_dirs"] = lists.obstacle_dirs ^ np.uint16(2)

@@ -85,3 +85,43 @@ def test_cuda_policy_matches_serial_policy_cylinder_with_analyzer(tmp_path):
     np.testing.assert_array_equal(outs["cuda"]["u"], outs["serial"]["u"])
     assert len(outs["serial"]["lift_drag"]) == 2 * 39
     np.testing.assert_array_equal(outs["cuda"]["lift_drag"], outs["serial"]["lift_drag"])
+
+
+def ps_cavity(n=64, r=7):
+    t = H.cavity_types(n)
+    ii, jj = np.mgrid[0:n, 0:n]
+    t[((ii - n // 2) ** 2 + (jj - n // 2) ** 2 <= r * r) & (t == H.FLUID)] = H.OBSTACLE
+    return t
+
+
+@needs_bins
+def test_serial_ps_example_matches_oracle(tmp_path):
+    """PSBounceBackPolicy obstacle (test/unit/LidWithPSObstacle.cpp's set-up,
+    compute_obstacle_weight included) through the reference's SerialPolicy."""
+    types = ps_cavity()
+    lists = H.classify(types)
+    lat = str(tmp_path / "ps.txt")
+    H.write_lattice_file(lat, types)
+    out = run("lid_ps_obstacle_serial", [lat, "300", "0.6", "0.55", str(tmp_path / "s")], str(tmp_path / "s"))
+    p = H.Params.trt_magic(0.6, obstacle_bc=1, ps_tau=0.55)
+    ref = H.run_oracle(lists, p, 300, H.open_values(lists, "lidramp:0.1:0.002", "const:0:0", 300))
+    act = active_flat(lists)
+    np.testing.assert_array_equal(out["populations"][act], ref["populations"].reshape(-1)[act])
+    np.testing.assert_array_equal(out["u"], ref["u"].reshape(-1))
+
+
+@needs_bins
+@pytest.mark.gpu
+def test_cuda_policy_matches_serial_policy_ps_obstacle(tmp_path):
+    types = ps_cavity(96, 10)
+    lists = H.classify(types)
+    lat = str(tmp_path / "ps.txt")
+    H.write_lattice_file(lat, types)
+    outs = {}
+    for pol in ("serial", "cuda"):
+        d = str(tmp_path / pol)
+        outs[pol] = run(f"lid_ps_obstacle_{pol}", [lat, "800", "0.6", "0.55", d], d)
+    act = active_flat(lists)
+    np.testing.assert_array_equal(outs["cuda"]["populations"][act], outs["serial"]["populations"][act])
+    np.testing.assert_array_equal(outs["cuda"]["u"], outs["serial"]["u"])
+    np.testing.assert_array_equal(outs["cuda"]["rho"], outs["serial"]["rho"])

@@ -19,7 +19,8 @@ def make_gpu(lists: H.NodeLists, p: H.Params, storage=0, table_rows=1, pipeline=
                          lists.outlet, lists.outlet_side, lists.obstacle, lists.obstacle_dirs,
                          collision=p.collision, tau=p.tau, tau_even=p.tau_even, tau_odd=p.tau_odd,
                          inlet_bc=p.inlet_bc, outlet_bc=p.outlet_bc, storage=storage,
-                         open_table_rows=table_rows)
+                         open_table_rows=table_rows, obstacle_bc=p.obstacle_bc, ps_tau=p.ps_tau,
+                         obstacle_b=p.obstacle_b)
     if pipeline is not None:
         g.set_pipeline(pipeline)
     return g

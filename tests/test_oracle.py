@@ -23,7 +23,8 @@ def params_from_args(args):
     a = dict(zip(args[::2], args[1::2]))
     bc = {"zh": H.BC_ZH_VELOCITY, "open": H.BC_OPEN, "zhp": H.BC_ZH_PRESSURE}
     kw = dict(inlet_bc=bc[a.get("--inlet", "zh")], outlet_bc=bc[a.get("--outlet", "zh")],
-              rho_out=float(a.get("--rho-out", 1.0)))
+              rho_out=float(a.get("--rho-out", 1.0)),
+              obstacle_bc=1 if a.get("--obstacle", "bb") == "ps" else 0, ps_tau=float(a.get("--ps-tau", 0.6)))
     if a.get("--collision", "bgk") == "trt":
         p = H.Params.trt_magic(float(a["--tau-even"]), float(a.get("--magic", 0.25)), **kw)
     else:
@@ -101,6 +102,7 @@ needs_ref = pytest.mark.skipif(not H.have_ref(), reason="oracle/_ref/ref_runner 
 
 
 def ref_vs_oracle(types, args, steps, tmp_path, extra=()):
+    tmp_path.mkdir(parents=True, exist_ok=True)
     path = str(tmp_path / "lattice.txt")
     H.write_lattice_file(path, types)
     res = H.run_ref(["--lattice-file", path, *args, "--steps", str(steps), "--dump-nodes", *extra],
@@ -142,3 +144,22 @@ def test_live_reference_lid_ramp(tmp_path):
     ref_vs_oracle(H.cavity_types(40), ["--collision", "trt", "--tau-even", "0.58", "--magic", "0.25",
                                        "--inlet", "zh", "--outlet", "zh", "--inlet-u", "lidramp:0.15:0.001"],
                   250, tmp_path)
+
+
+@needs_ref
+@pytest.mark.parametrize("coll", ["bgk", "trt"])
+def test_live_reference_partially_saturated_obstacles(coll, tmp_path):
+    """PSBounceBackPolicy on wet obstacles (walls keep plain bounce-back): a
+    channel with discs and a pressure outlet, and a cavity with a disc as in
+    test/unit/LidWithPSObstacle.cpp.  The oracle equals the reference bit for
+    bit."""
+    col = (["--collision", "bgk", "--tau", "0.7"] if coll == "bgk" else
+           ["--collision", "trt", "--tau-even", "0.6", "--magic", "0.25"])
+    ch = H.channel_types(40, 90, discs=[(20, 30, 7), (12, 62, 4)])
+    ref_vs_oracle(ch, col + ["--obstacle", "ps", "--ps-tau", "0.55", "--inlet", "zh", "--outlet", "zhp",
+                             "--inlet-u", "parabolic:0.04:1:38", "--outlet-u", "pressure"], 160, tmp_path / "ch")
+    cav = H.cavity_types(48)
+    ii, jj = np.mgrid[0:48, 0:48]
+    cav[((ii - 24) ** 2 + (jj - 24) ** 2 <= 64) & (cav == H.FLUID)] = H.OBSTACLE
+    ref_vs_oracle(cav, col + ["--obstacle", "ps", "--ps-tau", "0.51", "--inlet", "zh", "--outlet", "zh",
+                              "--inlet-u", "lidramp:0.1:0.002"], 200, tmp_path / "cav")
