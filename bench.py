@@ -437,6 +437,54 @@ def run_ours(a, dist):
     return line, wl, types
 
 
+def output_writer(L, device, size=1024, every=1000, saves=4):
+    """Saves of u on output steps (perform_lbm's write_lattice_file,
+    Lattice.hpp:370-374) on a size x size lid cavity: steps with the macro
+    output on the save steps and no files, the same run writing each file
+    before stepping on (the reference's order: copy, format, write), and the
+    same run through the asynchronous writer (the copy enqueued on the
+    lattice's stream, files written by native threads while the next steps
+    run; the final flush is inside the timed region)."""
+    import shutil
+    import tempfile
+
+    wl = workload("cavity", size)
+    types = wl["types"]()
+    nodes = L.classify(types)
+    R, C = types.shape
+    out = {"lattice": f"cavity{size}", "steps_between_saves": every, "saves": saves}
+    tmp = tempfile.mkdtemp(prefix="llb_out_")
+    try:
+        for mode in ("none", "sync", "async"):
+            g = make_lattice(L, wl, nodes, R, C, 0, device)
+            w = L.OutputWriter(tmp) if mode != "none" else None
+            g.init()
+            g.step(50)
+            g.synchronize()
+            t0 = time.perf_counter()
+            for n in range(saves):
+                g.step(every - 1)
+                g.step(1, macro=True)
+                if w:
+                    w.save_u(g, n)
+                    if mode == "sync":
+                        w.flush()
+            if w:
+                w.flush()
+            g.synchronize()
+            s = time.perf_counter() - t0
+            out[f"mlups_{mode}"] = round(R * C * every * saves / s / 1e6, 1)
+            if w:
+                st = w.stats()
+                out[f"write_s_per_file_{mode}"] = round(st["write_s"] / max(st["files"], 1), 4)
+                w.close()
+            g.close()
+        out["file_bytes"] = sum(os.path.getsize(os.path.join(tmp, f)) for f in os.listdir(tmp)) // (2 * saves)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 def batch_add(b, L, prob, storage):
     """Adds one config-4 problem to a batch (or creates it alone when b is None)."""
     types = prob["make_types"]()
@@ -778,6 +826,9 @@ def main():
                           "f64_plain_sequential": {k: sv["plain_f64_sequential"][k] for k in ("mlups", "busy_mlups",
                                                                                               "latency_s")},
                           "mlups_ratio": sv["mlups_ratio"], "capacity_ratio": sv["capacity_ratio"]}
+    if dist.world == 1 and a.workload == "porous4096" and not a.no_extras:
+        import llalbm_cuda as L
+        line["output_writer"] = output_writer(L, dist.local)
     if dist.rank == 0:
         if dist.world == 1 and not a.no_cpu_baseline:
             cb = reference_cpu(wl, types, 1, 3 if a.workload == "porous4096" else 100)

@@ -226,7 +226,8 @@ int llb_mass_momentum(llb_handle h, double out[3]);
    writer serves one calling thread at a time; flush (or destroy) the writer
    before destroying a lattice whose copies are still queued. */
 typedef struct llb_writer* llb_writer_handle;
-/* slots in [1, 64] (0: 3); threads in [1, 256] (0: up to 8 host threads). */
+/* slots in [1, 64] (0: 3); threads in [1, 256] (0: the host's hardware
+   threads, at most 16). */
 int llb_writer_create(const char* dir, int32_t slots, int32_t threads, llb_writer_handle* out);
 int llb_writer_save_u(llb_writer_handle w, llb_handle h, int64_t index);
 /* The same files from a host array u in the reference's (R, C, 2) column-major

@@ -8,13 +8,12 @@
 // event, formats the rows on a few threads and writes the two files.  The
 // reference writes each value with `ostream << double` (default flags,
 // precision 6, i.e. printf "%.6g" in the C locale) followed by a space, and
-// ends each lattice row with std::endl; std::to_chars with
-// chars_format::general and precision 6 is specified as that same printf
-// conversion, so the bytes are identical.
+// ends each lattice row with std::endl; put_g6 below produces those bytes.
 #include <algorithm>
 #include <cerrno>
 #include <charconv>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
@@ -37,6 +36,10 @@ double now_s() {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+}  // namespace
+
+namespace llb_out {
+
 struct Slot {
     double* buf = nullptr;  // host memory, (R, C, 2) column-major
     size_t cap = 0;         // doubles
@@ -49,7 +52,9 @@ struct Slot {
     bool busy = false;
 };
 
-}  // namespace
+}  // namespace llb_out
+
+using llb_out::Slot;
 
 struct llb_writer {
     std::string dir;
@@ -67,6 +72,7 @@ struct llb_writer {
     int64_t files = 0;
     double wait_s = 0.0, write_s = 0.0;
     std::vector<std::string> bx, by;  // per formatting thread: rows of u_x, u_y
+    std::vector<std::vector<double>> bt;  // per formatting thread: its band, row-major
 };
 
 namespace {
@@ -76,23 +82,122 @@ int wfail(llb_writer_handle w, int rc, const std::string& msg) {
     return rc;
 }
 
-// Rows [i0, i1) of component files: value, space; newline after each row.
-void format_rows(const double* u, int64_t R, int64_t C, int64_t i0, int64_t i1, std::string& sx, std::string& sy) {
-    sx.clear();
-    sy.clear();
-    const int64_t N = R * C;
-    char tmp[64];
-    for (int64_t i = i0; i < i1; ++i) {
-        for (int d = 0; d < 2; ++d) {
-            std::string& s = d == 0 ? sx : sy;
-            const double* col = u + d * N + i;
-            for (int64_t j = 0; j < C; ++j) {
-                const auto r = std::to_chars(tmp, tmp + sizeof(tmp) - 1, col[j * R], std::chars_format::general, 6);
-                *r.ptr = ' ';
-                s.append(tmp, r.ptr + 1);
+// printf "%.6g" of v (the reference's `ostream << double`).  The six
+// significant digits come from the exact binary value: v = m 2^e, so
+// m 10^k 2^e with k = 5 - X (X the decimal exponent) is split into its
+// integer part q and remainder r with 128-bit integer arithmetic, and q is
+// rounded to nearest, ties to even, as printf does.  Values outside the
+// fast range (|v| >= 2^52 or X outside [-17, 5], zero, subnormal, inf, nan)
+// go through std::to_chars, which the C++ standard specifies as that same
+// printf conversion.
+using u128 = unsigned __int128;
+
+struct Pow10 {
+    u128 p[23];
+    double d[48];  // 10^(x - 24) as doubles, for the first guess of X
+    Pow10() {
+        p[0] = 1;
+        for (int k = 1; k < 23; ++k) p[k] = p[k - 1] * 10u;
+        for (int x = 0; x < 48; ++x) d[x] = std::pow(10.0, x - 24);
+    }
+};
+const Pow10 kPow10;
+
+char* put_g6_slow(double v, char* p, char* end) {
+    return std::to_chars(p, end, v, std::chars_format::general, 6).ptr;
+}
+
+char* put_g6(double v, char* p, char* end) {
+    uint64_t bits;
+    std::memcpy(&bits, &v, sizeof(bits));
+    const int be = static_cast<int>((bits >> 52) & 0x7ff);
+    if (be == 0 || be == 0x7ff) return put_g6_slow(v, p, end);
+    const uint64_t m = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+    const int s = 1075 - be;  // v = m 2^-s
+    if (s <= 0 || s >= 128) return put_g6_slow(v, p, end);
+    // floor(log10 |v|) is X0 or X0 + 1; a comparison picks one, and the
+    // exact test below corrects the guess near a power of ten
+    int X = static_cast<int>(std::floor((be - 1023) * 0.30102999566398120));
+    if (X >= -24 && X < 23 && std::fabs(v) >= kPow10.d[X + 25]) ++X;
+    uint64_t N = 0;
+    for (int it = 0; it < 4 && !N; ++it) {
+        const int k = 5 - X;
+        if (k < 0 || k > 22) return put_g6_slow(v, p, end);
+        const u128 prod = static_cast<u128>(m) * kPow10.p[k];
+        u128 q = prod >> s;
+        const u128 r = prod - (q << s);
+        const u128 half = static_cast<u128>(1) << (s - 1);
+        if (q >= 1000000u) { ++X; continue; }  // X was one too small
+        if (q < 100000u) { --X; continue; }    // one too large
+        if (r > half || (r == half && (q & 1u))) ++q;
+        if (q == 1000000u) { q = 100000u; ++X; }  // rounded up to the next power of ten
+        N = static_cast<uint64_t>(q);
+    }
+    if (!N) return put_g6_slow(v, p, end);
+    char d[6];
+    for (int i = 5; i >= 0; --i) { d[i] = static_cast<char>('0' + N % 10); N /= 10; }
+    int nd = 6;
+    while (nd > 1 && d[nd - 1] == '0') --nd;
+    if (bits >> 63) *p++ = '-';
+    if (X >= -4 && X < 6) {
+        if (X >= 0) {
+            for (int i = 0; i <= X; ++i) *p++ = d[i];
+            if (nd > X + 1) {
+                *p++ = '.';
+                for (int i = X + 1; i < nd; ++i) *p++ = d[i];
             }
-            s.push_back('\n');
+        } else {
+            *p++ = '0';
+            *p++ = '.';
+            for (int i = 0; i < -X - 1; ++i) *p++ = '0';
+            for (int i = 0; i < nd; ++i) *p++ = d[i];
         }
+    } else {
+        *p++ = d[0];
+        if (nd > 1) {
+            *p++ = '.';
+            for (int i = 1; i < nd; ++i) *p++ = d[i];
+        }
+        *p++ = 'e';
+        *p++ = X < 0 ? '-' : '+';
+        const int ax = X < 0 ? -X : X;  // 5..17 here
+        *p++ = static_cast<char>('0' + ax / 10);
+        *p++ = static_cast<char>('0' + ax % 10);
+    }
+    return p;
+}
+
+// Rows [i0, i1) of both component files: value, space; newline after each
+// row.  u is column-major (a row's values lie R apart), so the band is first
+// transposed tile by tile into t (row-major) and then formatted in order.
+void format_rows(const double* u, int64_t R, int64_t C, int64_t i0, int64_t i1, std::string& sx, std::string& sy,
+                 std::vector<double>& t) {
+    constexpr int64_t TILE = 32;
+    const int64_t N = R * C, B = i1 - i0;
+    t.resize(static_cast<size_t>(2 * B * C));
+    for (int d = 0; d < 2; ++d)
+        for (int64_t jb = 0; jb < C; jb += TILE)
+            for (int64_t ib = i0; ib < i1; ib += TILE) {
+                const int64_t je = std::min(C, jb + TILE), ie = std::min(i1, ib + TILE);
+                for (int64_t j = jb; j < je; ++j) {
+                    const double* src = u + d * N + j * R;
+                    double* dst = t.data() + d * B * C + j;
+                    for (int64_t i = ib; i < ie; ++i) dst[(i - i0) * C] = src[i];
+                }
+            }
+    for (int d = 0; d < 2; ++d) {
+        std::string& s = d == 0 ? sx : sy;
+        s.resize(static_cast<size_t>(B * (C * 14 + 1)));  // at most 13 characters and a space per value
+        char* p = s.data();
+        const double* row = t.data() + d * B * C;
+        for (int64_t i = 0; i < B; ++i, row += C) {
+            for (int64_t j = 0; j < C; ++j) {
+                p = put_g6(row[j], p, p + 32);
+                *p++ = ' ';
+            }
+            *p++ = '\n';
+        }
+        s.resize(static_cast<size_t>(p - s.data()));
     }
 }
 
@@ -103,6 +208,7 @@ std::string write_slot(llb_writer* w, const Slot& s) {
     if (static_cast<int>(w->bx.size()) < T) {
         w->bx.resize(T);
         w->by.resize(T);
+        w->bt.resize(T);
     }
     auto rows = [&](int t) { return std::make_pair(R * t / T, R * (t + 1) / T); };
     std::vector<std::thread> pool;
@@ -110,11 +216,11 @@ std::string write_slot(llb_writer* w, const Slot& s) {
     for (int t = 1; t < T; ++t)
         pool.emplace_back([&, t] {
             const auto [a, b] = rows(t);
-            format_rows(s.buf, R, C, a, b, w->bx[t], w->by[t]);
+            format_rows(s.buf, R, C, a, b, w->bx[t], w->by[t], w->bt[t]);
         });
     {
         const auto [a, b] = rows(0);
-        format_rows(s.buf, R, C, a, b, w->bx[0], w->by[0]);
+        format_rows(s.buf, R, C, a, b, w->bx[0], w->by[0], w->bt[0]);
     }
     for (auto& th : pool) th.join();
     for (int d = 0; d < 2; ++d) {
@@ -233,7 +339,7 @@ int llb_writer_create(const char* dir, int32_t slots, int32_t threads, llb_write
     w->dir = dir;
     w->slots.resize(slots ? slots : 3);
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    w->nthreads = threads ? threads : static_cast<int>(std::min(8u, hw));
+    w->nthreads = threads ? threads : static_cast<int>(std::min(16u, hw));
     w->io = std::thread(io_loop, w);
     *out = w;
     return LLB_OK;

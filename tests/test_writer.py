@@ -36,17 +36,21 @@ def read_pair(directory, n):
 
 
 def sample_values(rng, shape):
-    u = rng.standard_normal(shape) * 10.0 ** rng.integers(-12, 12, shape)
+    """Magnitudes 1e-25..1e13 (both the writer's integer fast path and its
+    fallback), exact ties of the sixth digit, powers of ten and their
+    neighbours, tiny, huge and subnormal values, signed zeros."""
+    u = rng.standard_normal(shape) * 10.0 ** rng.integers(-25, 13, shape)
     flat = u.reshape(-1)
-    special = [0.0, -0.0, 1.0, -1.0, 0.1, 1e-5, 9.999995e-5, 123456.5, 1234567.0, 0.5e-4, 1e300, -1e-300,
-               2.5, 1.0 / 3.0, 999999.5, 9.9999995]
+    special = [0.0, -0.0, 1.0, -1.0, 0.1, 1e-5, 9.999995e-5, 123456.5, 123457.5, 1234567.0, 0.5e-4, 1e300,
+               -1e-300, 5e-324, 2.5, 1.0 / 3.0, 999999.5, 9.9999995, 0.0001, 0.00001, 1e-17, 1e-18, 99999.95,
+               np.nextafter(1e-4, 0.0), np.nextafter(1e6, 0.0), np.nextafter(1e6, 2e6), 2.0 ** -20, 3 * 2.0 ** -30]
     flat[: len(special)] = special
     return u
 
 
 def test_format_matches_printf(tmp_path):
     rng = np.random.default_rng(3)
-    u = sample_values(rng, (37, 53, 2))
+    u = sample_values(rng, (157, 211, 2))
     with L.OutputWriter(str(tmp_path), slots=2, threads=4) as w:
         w.save_host(u, 7)
         w.flush()
