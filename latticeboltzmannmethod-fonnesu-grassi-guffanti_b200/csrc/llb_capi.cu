@@ -73,6 +73,10 @@ LaunchCtx make_ctx(llb_handle h) {
     x.g.ps = h->d_ps;
     x.g.psb = h->d_psb;
     x.g.open_idx = h->d_open_idx;
+    x.g.sectors = h->tma_cfg == PIPE_LIST ? h->d_sectors : nullptr;
+    x.g.smask = h->d_smask;
+    x.g.sbb = h->d_sbb;
+    x.g.n_sectors = h->n_sectors;
     x.ot.vals = h->d_open;
     x.ot.n_open = h->n_open;
     x.ot.cap = h->cap;
@@ -93,7 +97,7 @@ void release(llb_handle h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& g : h->graph)
         if (g) cudaGraphExecDestroy(g);
-    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_ps, h->d_psb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
+    void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_ps, h->d_psb, h->d_sectors, h->d_smask, h->d_sbb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
                     h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -479,7 +483,6 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     // fastest measured on the 4096^2 porous channel, or one thread per node
     h->tma_cfg = prefers_tma(*h) ? (d->storage == LLB_STORE_F64 ? 1 : 0) : -1;
     if (!ps.empty()) h->tma_cfg = -1;  // partially saturated obstacles: one thread per node only
-
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete h; return fail(nullptr, LLB_E_NODEVICE, "no CUDA device"); }
     if (d->device < 0 || d->device >= ndev) { delete h; return fail(nullptr, LLB_E_NODEVICE, "device ordinal out of range"); }
@@ -752,13 +755,76 @@ int llb_event_elapsed_ms(llb_handle h, int32_t a, int32_t b, float* ms) {
     return LLB_OK;
 }
 
+// The active-sector list of a lattice (built on first use): every 32-byte
+// sector of a population plane holding an active node, ordered by tiles of
+// 32 rows x 8 columns (the one-thread grid's block) and column by column
+// inside a tile, with the mask and bounce bytes of the listed nodes.
+static int build_sector_list(llb_handle h) {
+    if (h->d_sectors) return LLB_OK;
+    if (h->d_ps) return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
+    if (static_cast<int64_t>(h->ld) * h->C >= (1LL << 31))
+        return fail(h, LLB_E_UNSUPPORTED, "no active-sector list for 2^31 or more slots per plane");
+    const size_t n = static_cast<size_t>(h->ld) * h->C;
+    std::vector<uint8_t> mask(n), bb(n);
+    LLB_CUDA(h, cudaMemcpyAsync(mask.data(), h->d_mask, n, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaMemcpyAsync(bb.data(), h->d_bb, n, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    const int64_t SN = LIST_BYTES / static_cast<int64_t>(h->elem), ld = h->ld;
+    std::vector<int32_t> sectors;
+    for (int64_t j0 = 0; j0 < h->C; j0 += 8)
+        for (int64_t i0 = 0; i0 < ld; i0 += 32)
+            for (int64_t j = j0; j < std::min<int64_t>(j0 + 8, h->C); ++j)
+                for (int64_t base = j * ld + i0; base < j * ld + std::min<int64_t>(i0 + 32, ld); base += SN) {
+                    bool any = false;
+                    for (int64_t q = 0; q < SN; ++q) any |= class_active(mask_class(mask[static_cast<size_t>(base + q)]));
+                    if (any) sectors.push_back(static_cast<int32_t>(base / SN));
+                }
+    if (sectors.empty()) return fail(h, LLB_E_UNSUPPORTED, "no active node");
+    std::vector<uint8_t> smask(sectors.size() * SN), sbb(sectors.size() * SN);
+    for (size_t e = 0; e < sectors.size(); ++e)
+        for (int64_t q = 0; q < SN; ++q) {
+            const size_t node = static_cast<size_t>(sectors[e]) * SN + q;
+            smask[e * SN + q] = mask[node];
+            sbb[e * SN + q] = bb[node];
+        }
+    // the handle takes the three buffers only when all of them are filled
+    int32_t* d_sec = nullptr;
+    uint8_t *d_sm = nullptr, *d_sb = nullptr;
+    int rc = dev_alloc(h, &d_sec, sectors.size() * sizeof(int32_t));
+    if (!rc) rc = dev_alloc(h, &d_sm, smask.size());
+    if (!rc) rc = dev_alloc(h, &d_sb, sbb.size());
+    cudaError_t e = cudaSuccess;
+    if (!rc) e = cudaMemcpyAsync(d_sec, sectors.data(), sectors.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess) e = cudaMemcpyAsync(d_sm, smask.data(), smask.size(), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess) e = cudaMemcpyAsync(d_sb, sbb.data(), sbb.size(), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(h, e, "active-sector list upload");
+    if (rc) {
+        const size_t sizes[3] = {sectors.size() * sizeof(int32_t), smask.size(), sbb.size()};
+        void* bufs[3] = {d_sec, d_sm, d_sb};
+        for (int q = 0; q < 3; ++q)
+            if (bufs[q]) {
+                cudaFree(bufs[q]);
+                h->bytes -= static_cast<int64_t>(sizes[q]);
+            }
+        return rc;
+    }
+    h->d_sectors = d_sec;
+    h->d_smask = d_sm;
+    h->d_sbb = d_sb;
+    h->n_sectors = static_cast<int>(sectors.size());
+    return LLB_OK;
+}
+
 int llb_set_pipeline(llb_handle h, int32_t config) {
-    if (!h || config < -1 || config >= TMA_CONFIGS) return fail(h, LLB_E_INVALID, "config must be -1 or in [0, 3)");
-    if (config >= 0 && h->d_ps)
+    if (!h || config < PIPE_LIST || config >= TMA_CONFIGS)
+        return fail(h, LLB_E_INVALID, "config must be -2, -1 or in [0, 3)");
+    if (config != PIPE_GRID && h->d_ps)
         return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
     if (config != h->tma_cfg) {
         int rc = select_device(h);
         if (rc) return rc;
+        if (config == PIPE_LIST && (rc = build_sector_list(h))) return rc;
         LLB_CUDA(h, cudaStreamSynchronize(h->stream));
         for (auto& g : h->graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }

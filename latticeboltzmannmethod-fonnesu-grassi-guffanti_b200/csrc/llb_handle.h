@@ -30,6 +30,10 @@ struct llb_lattice {
     uint8_t* d_bb = nullptr;
     uint8_t* d_ps = nullptr;   // partially saturated obstacles only
     double* d_psb = nullptr;
+    int32_t* d_sectors = nullptr;  // active-sector list (lattices of fewer than 2^31 slots per plane)
+    uint8_t* d_smask = nullptr;    // mask and bounce bytes of the listed nodes
+    uint8_t* d_sbb = nullptr;
+    int n_sectors = 0;
     int32_t* d_open_idx = nullptr;
     double2* d_open = nullptr;
     int n_open = 0, cap = 1;
@@ -54,8 +58,8 @@ struct llb_lattice {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t bytes = 0;
     std::string err;
-    // TMA-pipelined step kernel (plain steps); tma_cfg < 0 selects the
-    // one-thread-per-node kernel.
+    // plain-step kernel: tma_cfg >= 0 the TMA pipeline configuration,
+    // PIPE_GRID the one-thread-per-node grid, PIPE_LIST the active-sector list
     int tma_cfg = 0;
     TmaPlan plan;
     bool maps_ready = false;
@@ -72,6 +76,7 @@ struct llb_lattice {
 // the rest (it reads only active nodes and runs close to the copy bandwidth
 // on open flow).  Measured on B200 for cavities, channels and porous media
 // from 224^2 to 4096^2.
+constexpr int PIPE_GRID = -1, PIPE_LIST = -2;
 constexpr int64_t TMA_MIN_NODES = 1 << 19;
 constexpr double TMA_MIN_NONPLAIN = 0.05;
 inline bool prefers_tma(const llb_lattice& h) {

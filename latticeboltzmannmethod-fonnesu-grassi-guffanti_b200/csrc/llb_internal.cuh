@@ -72,6 +72,9 @@ __host__ __device__ constexpr float w_f32(int k) { return k == 0 ? 4.0f / 9.0f :
 // ---- kernel parameters ------------------------------------------------------
 constexpr int MAX_BLOCK_Y = 8;  // columns per block of the step kernel, at most
 
+// Bytes of a population plane per entry of the active-sector list.
+constexpr int LIST_BYTES = 32;
+
 struct Geometry {
     int rows, cols;     // R, C
     int ld;             // column stride (elements) of populations / mask / open_idx
@@ -83,6 +86,13 @@ struct Geometry {
     const uint8_t* __restrict__ ps;
     const double* __restrict__ psb;
     const int32_t* __restrict__ open_idx;
+    // active-sector list of the plain steps (NULL: the one-thread-per-node
+    // grid): ids of the 32-byte sectors of a population plane that hold an
+    // active node
+    const int32_t* __restrict__ sectors;
+    const uint8_t* __restrict__ smask;  // mask byte of each listed node (sector order)
+    const uint8_t* __restrict__ sbb;    // bounce byte of each listed node
+    int n_sectors;
 };
 
 struct OpenTable {

@@ -31,6 +31,13 @@ cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, 
         }
     }
 #undef LLB_STEP_PS
+    if (!init && !macro && x.g.sectors && x.g.n_sectors > 0) {  // plain step over the active-sector list
+        const long long threads = static_cast<long long>(x.g.n_sectors) * (LIST_BYTES / static_cast<int>(sizeof(T)));
+        const unsigned blocks = static_cast<unsigned>((threads + LIST_BLOCK - 1) / LIST_BLOCK);
+        if (x.c.model == 0) k_step_list<M, 0><<<blocks, LIST_BLOCK, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss);
+        else k_step_list<M, 1><<<blocks, LIST_BLOCK, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss);
+        return cudaGetLastError();
+    }
     if (x.c.model == 0) {
         if (init) { if (macro) LLB_STEP(0, true, true); else LLB_STEP(0, false, true); }
         else { if (macro) LLB_STEP(0, true, false); else LLB_STEP(0, false, false); }

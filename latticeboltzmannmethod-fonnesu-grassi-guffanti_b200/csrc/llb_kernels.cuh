@@ -30,15 +30,18 @@ constexpr int BX = 32, BY = MAX_BLOCK_Y;  // one warp = 32 rows of one column
 // Such warps read straight from the sources; the others take one branch-free
 // path on every lane, where a bounce-back source is only another address
 // (plain lanes skip the bounce-bit load).
+// b_pre: the node's bounce byte when the caller has it already (NO_BB: load it).
+constexpr unsigned NO_BB = 0x100u;
 template <class M>
 __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __restrict__ fin, int i, int j,
-                                     long long node, uint8_t m, bool warp_plain, typename M::R* f) {
+                                     long long node, uint8_t m, bool warp_plain, typename M::R* f,
+                                     unsigned b_pre = NO_BB) {
     f[0] = M::load(fin + node);
     if (warp_plain) {
 #pragma unroll
         for (int k = 1; k < 9; ++k) f[k] = M::load(fin + k * g.plane + node - (DJ(k) * g.ld + DI(k)));
     } else if (i > 0 && j > 0 && i < g.rows - 1 && j < g.cols - 1) {
-        const unsigned b = (m & MASK_PLAIN) ? 0u : g.bb[node];
+        const unsigned b = (m & MASK_PLAIN) ? 0u : (b_pre != NO_BB ? b_pre : g.bb[node]);
 #pragma unroll
         for (int k = 1; k < 9; ++k) {
             const typename M::T* p = ((b >> (k - 1)) & 1u) ? fin + opp(k) * g.plane + node
@@ -160,20 +163,21 @@ __device__ __forceinline__ void ps_push(const Geometry& g, T* __restrict__ fout,
     }
 }
 
+// One node of a step (steps 1-4 above).  Every lane of the warp calls it
+// (warp votes inside).  inside: (i, j) is a node of the lattice, m its mask;
+// write_sector: the node's 32-byte sector holds an active node, so an
+// inactive node of it stores the initial values; padding: (i, j) is a padding
+// row of a column (rows <= i < ld), stored like a dead node; b_pre: the
+// node's bounce byte if already loaded (NO_BB otherwise).
 // INIT == true: step 0 from the initial equilibrium (Lattice.hpp:326-328).
-// Block: 32 rows (one warp per column) x blockDim.y columns, blockDim.y <= BY.
-template <class M, int COLL, bool MACRO, bool INIT, bool PS = false>
-__global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Collision c,
-                                                 const typename M::T* __restrict__ fin,
-                                                 typename M::T* __restrict__ fout, MacroOut mo, StepSync ss) {
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+template <class M, int COLL, bool MACRO, bool INIT, bool PS>
+__device__ __forceinline__ void step_node(const Geometry& g, const OpenTable& ot, const Collision& c,
+                                          const typename M::T* __restrict__ fin, typename M::T* __restrict__ fout,
+                                          const MacroOut& mo, const StepSync& ss, int i, int j, long long node,
+                                          bool inside, uint8_t m, bool write_sector, bool padding,
+                                          unsigned b_pre = NO_BB) {
     bool bad = false;
-    const bool inside = i < g.rows && j < g.cols;
-    const long long node = static_cast<long long>(j) * g.ld + i;
-    const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
     const uint8_t cls = mask_class(m);
-    const bool write_sector = sector_has_active<M>(class_active(cls));
     const bool warp_plain = __all_sync(0xffffffffu, !(inside && class_active(cls)) || (m & MASK_PLAIN));
     if (inside) {
         if (class_active(cls)) {
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
 #pragma unroll
                 for (int k = 0; k < 9; ++k) f[k] = M::keep(k);
             } else {
-                pull<M>(g, fin, i, j, node, m, warp_plain, f);
+                pull<M>(g, fin, i, j, node, m, warp_plain, f, b_pre);
             }
             // moments stay in the model's arithmetic type up to the collision
             typename M::R rr, xr, yr;
@@ -231,12 +235,64 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
                 mo.u[d + N] = 0.0;
             }
         }
-    } else if (write_sector && j < g.cols && i < g.ld) {
+    } else if (write_sector && padding) {
         // padding rows (dead) of a column that shares a sector with active nodes
 #pragma unroll
         for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
     }
     flag_numerics(ss, bad);
+}
+
+// Block: 32 rows (one warp per column) x blockDim.y columns, blockDim.y <= BY.
+template <class M, int COLL, bool MACRO, bool INIT, bool PS = false>
+__global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Collision c,
+                                                 const typename M::T* __restrict__ fin,
+                                                 typename M::T* __restrict__ fout, MacroOut mo, StepSync ss) {
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool inside = i < g.rows && j < g.cols;
+    const long long node = static_cast<long long>(j) * g.ld + i;
+    const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
+    const bool write_sector = sector_has_active<M>(class_active(mask_class(m)));
+    step_node<M, COLL, MACRO, INIT, PS>(g, ot, c, fin, fout, mo, ss, i, j, node, inside, m, write_sector,
+                                        j < g.cols && i < g.ld);
+}
+
+// Plain steps over the active-sector list: one thread per node of every
+// 32-byte sector of a population plane that holds an active node (the
+// sectors' ids in g.sectors; the listed nodes' mask and bounce bytes in
+// g.smask / g.sbb, so a thread's first loads are independent of each
+// other).  Sectors of obstacle interiors and dead regions are neither read
+// nor written, and every lane of a warp has a node to update or to complete
+// its sector, which the one-thread-per-node grid cannot give on porous
+// geometry (there a third of its lanes idle).  Same per-node arithmetic as
+// k_step.
+constexpr int LIST_BLOCK = 256;
+template <class M, int COLL>
+__global__ void __launch_bounds__(LIST_BLOCK, 5) k_step_list(Geometry g, OpenTable ot, Collision c,
+                                                          const typename M::T* __restrict__ fin,
+                                                          typename M::T* __restrict__ fout, MacroOut mo,
+                                                          StepSync ss) {
+    constexpr int SN = LIST_BYTES / sizeof(typename M::T);  // nodes per listed block
+    const long long t = static_cast<long long>(blockIdx.x) * LIST_BLOCK + threadIdx.x;
+    const long long e = t / SN;
+    const bool valid = e < g.n_sectors;
+    long long node = 0;
+    int i = 0, j = 0;
+    uint8_t m = CLS_DEAD;
+    unsigned b = 0;
+    if (valid) {
+        m = g.smask[t];
+        b = g.sbb[t];
+        node = static_cast<long long>(g.sectors[e]) * SN + (t & (SN - 1));
+        // node < 2^31 for every lattice that has a list
+        const unsigned un = static_cast<unsigned>(node), uj = un / static_cast<unsigned>(g.ld);
+        j = static_cast<int>(uj);
+        i = static_cast<int>(un - uj * static_cast<unsigned>(g.ld));
+    }
+    // padding rows of a listed sector carry a dead mask: like a dead node of
+    // the lattice, they store the initial values
+    step_node<M, COLL, false, false, false>(g, ot, c, fin, fout, mo, ss, i, j, node, valid, m, valid, valid, b);
 }
 
 // Every slot of a population buffer set to the node-independent initial value

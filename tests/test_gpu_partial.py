@@ -63,9 +63,10 @@ def test_partially_saturated_limits():
     assert e.value.code == -8
     with L.CudaLattice(*args, **kw) as g:
         assert g.pipeline == -1
-        with pytest.raises(L.LLBError) as e:
-            g.set_pipeline(1)
-        assert e.value.code == -8
+        for cfg in (1, -2):
+            with pytest.raises(L.LLBError) as e:
+                g.set_pipeline(cfg)
+            assert e.value.code == -8
     with L.CudaBatch(storage=L.STORE_F64) as b:
         with pytest.raises(L.LLBError) as e:
             b.add(*args, **kw)
