@@ -358,10 +358,15 @@ int llb_event_record(llb_handle h, int32_t slot);
 int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, float* ms);
 /* Step-kernel selection, for the autotuner.  Plain steps run the TMA-pipelined
    kernel in configuration `config` (0..2: tile shape, stage count, warps), the
-   one-thread-per-node kernel for config -1, or for config -2 one thread per
-   node of every 32-byte population sector that holds an active node (a list
-   built by llb_create; lattices with partially saturated obstacles or 2^31 or
-   more slots per plane have none).  All compute identical arithmetic. */
+   two-steps-per-pass kernel (3..5: the intermediate step stays in shared
+   memory, so a pair of steps reads and writes the populations once; a lone
+   step runs on the one-thread kernel), the one-thread-per-node kernel for
+   config -1, or for config -2 one thread per node of every 32-byte population
+   sector that holds an active node (a list built on first use; lattices with
+   partially saturated obstacles or 2^31 or more slots per plane have none).
+   All compute the same per-node arithmetic: FP64 results are identical; the
+   shifted forms may differ in the last bits, as their kernels may contract
+   multiply-adds differently. */
 int llb_set_pipeline(llb_handle h, int32_t config);
 int llb_get_pipeline(llb_handle h, int32_t* config);
 /* Columns of lattice nodes per thread block of the one-thread-per-node kernel

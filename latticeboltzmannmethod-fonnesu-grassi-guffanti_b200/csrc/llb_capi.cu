@@ -272,9 +272,16 @@ int build_maps(llb_handle h) {
     return LLB_OK;
 }
 
-// One step kernel.  Inside a graph capture the step index is relative
-// (graph_offset >= 0, base read from d_step); otherwise it is absolute.
-int launch_one(llb_handle h, bool macro, long long graph_offset = -1) {
+// Steps one plain-step launch advances: 2 for the two-step configurations.
+int steps_per_launch(llb_handle h) {
+    TmaPlan p;
+    return h->tma_cfg >= 0 && tma_plan(h->storage, h->tma_cfg, &p) && p.pair ? 2 : 1;
+}
+
+// One step kernel (two steps for a two-step configuration unless `single`).
+// Inside a graph capture the step index is relative (graph_offset >= 0, base
+// read from d_step); otherwise it is absolute.
+int launch_one(llb_handle h, bool macro, long long graph_offset = -1, bool single = false) {
     LaunchCtx x = make_ctx(h);
     if (graph_offset >= 0) {
         x.ss.tbase = h->d_step;
@@ -283,14 +290,18 @@ int launch_one(llb_handle h, bool macro, long long graph_offset = -1) {
     if (!macro && h->tma_cfg >= 0) {
         int rc = build_maps(h);
         if (rc) return rc;
-        const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
-        const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
-        cudaError_t e = launch_step_tma(h->storage, h->plan, x, &h->pmap[h->cur], &h->mmap, h->f[h->cur],
-                                        h->f[h->cur ^ 1], grid);
-        if (e != cudaSuccess) return cuda_fail(h, e, "pipelined step kernel launch");
-        h->cur ^= 1;
-        ++h->step;
-        return LLB_OK;
+        if (!(h->plan.pair && single)) {
+            const long long ntiles =
+                ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
+            const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
+            cudaError_t e = launch_step_tma(h->storage, h->plan, x, &h->pmap[h->cur], &h->mmap, h->f[h->cur],
+                                            h->f[h->cur ^ 1], grid);
+            if (e != cudaSuccess) return cuda_fail(h, e, "pipelined step kernel launch");
+            h->cur ^= 1;
+            h->step += h->plan.pair ? 2 : 1;
+            return LLB_OK;
+        }
+        // a lone step of a two-step configuration: the one-thread-per-node kernel
     }
     cudaError_t e = launch_step(h->storage, x, h->f[h->cur], h->f[h->cur ^ 1], false, macro);
     if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
@@ -306,7 +317,8 @@ int graph_for(llb_handle h, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     LLB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int rc = LLB_OK;
-    for (int s = 0; s < GRAPH_STEPS && rc == LLB_OK; ++s) rc = launch_one(h, false, s);
+    const int per = steps_per_launch(h);
+    for (int s = 0; s < GRAPH_STEPS && rc == LLB_OK; s += per) rc = launch_one(h, false, s);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->cur = cur0;
     h->step = step0;
@@ -392,13 +404,13 @@ int handle_launch_step(llb_handle h, int cur, const long long* tbase, long long 
     x.ss.tbase = tbase;
     x.ss.t_off = t_off;
     cudaError_t e;
-    if (h->tma_cfg >= 0) {
+    if (h->tma_cfg >= 0 && steps_per_launch(h) == 1) {
         int rc = build_maps(h);
         if (rc) return rc;
         const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
         const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
         e = launch_step_tma(h->storage, h->plan, x, &h->pmap[cur], &h->mmap, h->f[cur], h->f[cur ^ 1], grid);
-    } else {
+    } else {  // one step at a time in a batch: a two-step configuration uses the one-thread kernel
         e = launch_step(h->storage, x, h->f[cur], h->f[cur ^ 1], false, false);
     }
     return e == cudaSuccess ? LLB_OK : cuda_fail(h, e, "step kernel launch");
@@ -585,8 +597,10 @@ int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
             plain -= GRAPH_STEPS;
         }
     }
-    for (int32_t s = 0; s < plain; ++s)
+    const int per = steps_per_launch(h);
+    for (; plain >= per; plain -= per)
         if ((rc = launch_one(h, false))) return rc;
+    if (plain > 0 && (rc = launch_one(h, false, -1, true))) return rc;
     if (macro) {
         if ((rc = launch_one(h, true))) return rc;
         h->macro_valid = true;
@@ -818,7 +832,7 @@ static int build_sector_list(llb_handle h) {
 
 int llb_set_pipeline(llb_handle h, int32_t config) {
     if (!h || config < PIPE_LIST || config >= TMA_CONFIGS)
-        return fail(h, LLB_E_INVALID, "config must be -2, -1 or in [0, 3)");
+        return fail(h, LLB_E_INVALID, "config must be -2, -1 or in [0, 6)");
     if (config != PIPE_GRID && h->d_ps)
         return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
     if (config != h->tma_cfg) {

@@ -29,12 +29,19 @@ cudaError_t launch_gather_forces_f64(const LaunchCtx& x, const void* fin, const 
 using F64Cfg0 = TmaCfg<double, 128, 4, 4, 16>;
 using F64Cfg1 = TmaCfg<double, 128, 8, 2, 16>;
 using F64Cfg2 = TmaCfg<double, 128, 4, 4, 20>;
+// two steps per launch (tile rows, tile columns, stages, consumer warps)
+using F64Pair3 = PairCfg<double, 32, 16, 2, 16>;
+using F64Pair4 = PairCfg<double, 32, 16, 3, 16>;
+using F64Pair5 = PairCfg<double, 64, 8, 2, 16>;
 
 bool tma_plan_f64(int cfg, TmaPlan* p) {
     switch (cfg) {
     case 0: fill_plan<ModelF64, F64Cfg0>(0, p); return true;
     case 1: fill_plan<ModelF64, F64Cfg1>(1, p); return true;
     case 2: fill_plan<ModelF64, F64Cfg2>(2, p); return true;
+    case 3: fill_plan<ModelF64, F64Pair3>(3, p); return true;
+    case 4: fill_plan<ModelF64, F64Pair4>(4, p); return true;
+    case 5: fill_plan<ModelF64, F64Pair5>(5, p); return true;
     default: return false;
     }
 }
@@ -45,6 +52,9 @@ cudaError_t launch_step_tma_f64(const TmaPlan& p, const LaunchCtx& x, const CUte
     case 0: return do_step_tma<ModelF64, F64Cfg0>(x, pm, mm, fin, fout, grid);
     case 1: return do_step_tma<ModelF64, F64Cfg1>(x, pm, mm, fin, fout, grid);
     case 2: return do_step_tma<ModelF64, F64Cfg2>(x, pm, mm, fin, fout, grid);
+    case 3: return do_step_pair<ModelF64, F64Pair3>(x, pm, mm, fin, fout, grid);
+    case 4: return do_step_pair<ModelF64, F64Pair4>(x, pm, mm, fin, fout, grid);
+    case 5: return do_step_pair<ModelF64, F64Pair5>(x, pm, mm, fin, fout, grid);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -4,6 +4,7 @@
 #include "llb_kernels.cuh"
 #include "llb_launch.h"
 #include "llb_tma.cuh"
+#include "llb_pair.cuh"
 #include "llb_batch.cuh"
 
 namespace llb {
@@ -96,6 +97,7 @@ cudaError_t do_gather(const LaunchCtx& x, const void* fin, const int64_t* pts, c
 template <class M, class CFG>
 void fill_plan(int cfg, TmaPlan* p) {
     p->cfg = cfg;
+    p->pair = CFG::PAIR;
     p->TI = CFG::TI;
     p->TJ = CFG::TJ;
     p->S = CFG::S;
@@ -114,6 +116,20 @@ cudaError_t do_step_tma(const LaunchCtx& x, const CUtensorMap* pmap, const CUten
     using T = typename M::T;
     auto k0 = k_step_tma<M, 0, CFG>;
     auto k1 = k_step_tma<M, 1, CFG>;
+    auto kern = x.c.model == 0 ? k0 : k1;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CFG::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, x.g, x.ot, x.c, static_cast<const T*>(fin),
+                                                             static_cast<T*>(fout), x.ss);
+    return cudaGetLastError();
+}
+
+template <class M, class CFG>
+cudaError_t do_step_pair(const LaunchCtx& x, const CUtensorMap* pmap, const CUtensorMap* mmap, const void* fin,
+                         void* fout, int grid) {
+    using T = typename M::T;
+    auto k0 = k_step_pair<M, 0, CFG>;
+    auto k1 = k_step_pair<M, 1, CFG>;
     auto kern = x.c.model == 0 ? k0 : k1;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CFG::SMEM_BYTES);
     if (e != cudaSuccess) return e;

@@ -85,6 +85,7 @@ cudaError_t launch_gather_forces_lowp(int storage, const LaunchCtx&, const void*
 // S shared-memory stages, W consumer warps + 1 producer warp).
 struct TmaPlan {
     int cfg = -1;
+    bool pair = false;     // two steps per launch (k_step_pair)
     int TI = 0, TJ = 0, S = 0, W = 0;
     int BI = 0;            // rows of a population box
     int BJ = 0;            // columns of a population box
@@ -92,7 +93,10 @@ struct TmaPlan {
     int smem = 0;          // dynamic shared memory bytes
     int threads = 0;
 };
-constexpr int TMA_CONFIGS = 3;
+// Configurations 0..2: one step per launch (k_step_tma); 3..5: two steps per
+// launch (k_step_pair).
+constexpr int TMA_CONFIGS = 6;
+constexpr int FIRST_PAIR_CONFIG = 3;
 // Fills `out` for configuration `cfg` (0..TMA_CONFIGS-1) of a storage form.
 bool tma_plan(int storage, int cfg, TmaPlan* out);
 cudaError_t launch_step_tma(int storage, const TmaPlan& p, const LaunchCtx& ctx, const CUtensorMap* pmap,

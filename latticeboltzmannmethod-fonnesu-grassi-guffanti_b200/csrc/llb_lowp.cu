@@ -45,6 +45,13 @@ using F32Cfg2 = TmaCfg<float, 128, 8, 4, 24>;
 using F16Cfg0 = TmaCfg<__half, 128, 24, 3, 24>;
 using F16Cfg1 = TmaCfg<__half, 128, 16, 3, 16>;
 using F16Cfg2 = TmaCfg<__half, 128, 32, 2, 16>;
+// two steps per launch
+using F32Pair3 = PairCfg<float, 32, 32, 2, 16>;
+using F32Pair4 = PairCfg<float, 32, 32, 3, 16>;
+using F32Pair5 = PairCfg<float, 64, 16, 2, 16>;
+using F16Pair3 = PairCfg<__half, 32, 64, 2, 16>;
+using F16Pair4 = PairCfg<__half, 64, 32, 2, 16>;
+using F16Pair5 = PairCfg<__half, 32, 32, 3, 16>;
 
 bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
     if (storage == LLB_STORE_F32S) {
@@ -52,6 +59,9 @@ bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
         case 0: fill_plan<ModelF32S, F32Cfg0>(0, p); return true;
         case 1: fill_plan<ModelF32S, F32Cfg1>(1, p); return true;
         case 2: fill_plan<ModelF32S, F32Cfg2>(2, p); return true;
+        case 3: fill_plan<ModelF32S, F32Pair3>(3, p); return true;
+        case 4: fill_plan<ModelF32S, F32Pair4>(4, p); return true;
+        case 5: fill_plan<ModelF32S, F32Pair5>(5, p); return true;
         default: return false;
         }
     }
@@ -59,6 +69,9 @@ bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
     case 0: fill_plan<ModelF16S, F16Cfg0>(0, p); return true;
     case 1: fill_plan<ModelF16S, F16Cfg1>(1, p); return true;
     case 2: fill_plan<ModelF16S, F16Cfg2>(2, p); return true;
+    case 3: fill_plan<ModelF16S, F16Pair3>(3, p); return true;
+    case 4: fill_plan<ModelF16S, F16Pair4>(4, p); return true;
+    case 5: fill_plan<ModelF16S, F16Pair5>(5, p); return true;
     default: return false;
     }
 }
@@ -70,6 +83,9 @@ cudaError_t launch_step_tma_lowp(int storage, const TmaPlan& p, const LaunchCtx&
         case 0: return do_step_tma<ModelF32S, F32Cfg0>(x, pm, mm, fin, fout, grid);
         case 1: return do_step_tma<ModelF32S, F32Cfg1>(x, pm, mm, fin, fout, grid);
         case 2: return do_step_tma<ModelF32S, F32Cfg2>(x, pm, mm, fin, fout, grid);
+        case 3: return do_step_pair<ModelF32S, F32Pair3>(x, pm, mm, fin, fout, grid);
+        case 4: return do_step_pair<ModelF32S, F32Pair4>(x, pm, mm, fin, fout, grid);
+        case 5: return do_step_pair<ModelF32S, F32Pair5>(x, pm, mm, fin, fout, grid);
         default: return cudaErrorInvalidValue;
         }
     }
@@ -77,6 +93,9 @@ cudaError_t launch_step_tma_lowp(int storage, const TmaPlan& p, const LaunchCtx&
     case 0: return do_step_tma<ModelF16S, F16Cfg0>(x, pm, mm, fin, fout, grid);
     case 1: return do_step_tma<ModelF16S, F16Cfg1>(x, pm, mm, fin, fout, grid);
     case 2: return do_step_tma<ModelF16S, F16Cfg2>(x, pm, mm, fin, fout, grid);
+    case 3: return do_step_pair<ModelF16S, F16Pair3>(x, pm, mm, fin, fout, grid);
+    case 4: return do_step_pair<ModelF16S, F16Pair4>(x, pm, mm, fin, fout, grid);
+    case 5: return do_step_pair<ModelF16S, F16Pair5>(x, pm, mm, fin, fout, grid);
     default: return cudaErrorInvalidValue;
     }
 }

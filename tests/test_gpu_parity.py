@@ -91,14 +91,17 @@ def test_f64_bit_exact(case, steps):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
+@pytest.mark.parametrize("pipeline", [-2, 3, 4, 5])
 @pytest.mark.parametrize("steps", [2, 7, 300])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-def test_f64_sector_list_bit_exact(case, steps):
-    """The active-sector list kernel (-2) on every case."""
+def test_f64_list_and_two_step_kernels_bit_exact(case, steps, pipeline):
+    """The active-sector list kernel (-2) and the two-steps-per-launch
+    configurations (3-5; odd step counts end with a lone step, 300 steps run
+    through graph replays) on every case."""
     name, lists, p, ins, outs = case
     table = H.open_values(lists, ins, outs, steps)
     ref = H.run_oracle(lists, p, steps, table)
-    got = run_gpu(lists, p, steps, table, pipeline=-2)
+    got = run_gpu(lists, p, steps, table, pipeline=pipeline)
     act = H.active_mask(lists)
     np.testing.assert_array_equal(got["populations"][:, act], ref["populations"][:, act])
     np.testing.assert_array_equal(got["post"][:, act], ref["post"][:, act])
@@ -106,7 +109,7 @@ def test_f64_sector_list_bit_exact(case, steps):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
-@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2])
+@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("case", [CASES[2], CASES[5], CASES[6]], ids=[CASES[2][0], CASES[5][0], CASES[6][0]])
 def test_f64_every_step_kernel_bit_exact(case, pipeline):
     """The active-sector list (-2), the one-thread-per-node kernel (-1) and
@@ -128,7 +131,7 @@ def test_f64_pipeline_large_lattice_bit_exact():
     p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
     table = H.open_values(lists, "const:0.02:0", "pressure", 1)
     outs = []
-    for pipeline in (-1, -2, 0, 1, 2):
+    for pipeline in (-1, -2, 0, 1, 2, 3, 4, 5):
         outs.append(run_gpu(lists, p, 60, table, pipeline=pipeline))
     act = H.active_mask(lists)
     for o in outs[1:]:
@@ -154,7 +157,7 @@ def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
-@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2])
+@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3)], ids=["f32s", "f16s"])
 def test_shifted_storage_velocity_error(storage, tol, pipeline):
     lists = H.classify(H.channel_types(64, 160, discs=[(32, 40, 8)]))
