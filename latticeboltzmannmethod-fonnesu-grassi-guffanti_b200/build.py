@@ -4,8 +4,9 @@
     python build.py --force    # rebuild everything
 
 The FP64 kernels (csrc/llb_f64.cu) are compiled with --fmad=false so their
-arithmetic rounds exactly like the reference's x86-64 build; the shifted
-low-precision kernels may contract multiply-adds.
+arithmetic rounds exactly like the reference's x86-64 build.  The shifted
+low-precision kernels (csrc/llb_lowp.cu) are compiled the same way and write
+their multiply-adds out (__fmaf_rn), so every kernel of a form rounds alike.
 """
 from __future__ import annotations
 
@@ -26,7 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I", CSR
 
 SOURCES = {
     "llb_f64.cu": ["--fmad=false"],
-    "llb_lowp.cu": [],
+    "llb_lowp.cu": ["--fmad=false"],
     "llb_capi.cu": [],
     "llb_noalloc.cu": [],
     "llb_batch.cu": [],

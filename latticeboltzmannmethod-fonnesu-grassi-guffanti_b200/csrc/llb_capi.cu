@@ -491,9 +491,7 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     int rc = build_mask(d, h->ld, mask, bb, ps, psb, open_idx, h->n_nonplain, why);
     if (rc != LLB_OK) { delete h; return fail(nullptr, rc, why); }
     h->n_active = d->n_fluid + d->n_inlet + d->n_outlet;
-    // default kernel: pipeline configuration 1 (FP64) or 0 (shifted forms), the
-    // fastest measured on the 4096^2 porous channel, or one thread per node
-    h->tma_cfg = prefers_tma(*h) ? (d->storage == LLB_STORE_F64 ? 1 : 0) : -1;
+    h->tma_cfg = default_pipeline(*h);
     if (!ps.empty()) h->tma_cfg = -1;  // partially saturated obstacles: one thread per node only
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete h; return fail(nullptr, LLB_E_NODEVICE, "no CUDA device"); }

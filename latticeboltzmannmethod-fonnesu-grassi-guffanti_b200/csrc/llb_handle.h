@@ -70,18 +70,31 @@ struct llb_lattice {
     int64_t n_active = 0, n_nonplain = 0;
 };
 
-// Default step kernel of a lattice: the TMA pipeline for large lattices with
-// many nodes next to obstacles (its bounce-back is a shared-memory address
-// select and its tiles stage every node), the one-thread-per-node kernel for
-// the rest (it reads only active nodes and runs close to the copy bandwidth
-// on open flow).  Measured on B200 for cavities, channels and porous media
-// from 224^2 to 4096^2.
+// Default plain-step kernel of a lattice, from measurements on B200 (cavities,
+// channels, cylinders and porous media from 724^2 to 4096^2, every storage
+// form):
+//  * below 2^19 nodes: one thread per node;
+//  * at least 5 % of the active nodes not PLAIN (porous media): the TMA
+//    pipeline -- FP64 configuration 1 from 2^21 nodes, else 0; configuration
+//    0 for the shifted forms (its bounce-back is a shared-memory address
+//    select, and its tiles stage every node);
+//  * open flow whose resident state (two buffers of 9 planes) exceeds the L2
+//    cache several times over: two steps per pass for FP64 and FP32
+//    (configuration 3, from 2^28 bytes), the TMA pipeline for FP16 (from 2^27
+//    bytes);
+//  * otherwise one thread per node, which reads only active sectors and runs
+//    close to the copy bandwidth on open flow.
 constexpr int PIPE_GRID = -1, PIPE_LIST = -2;
 constexpr int64_t TMA_MIN_NODES = 1 << 19;
 constexpr double TMA_MIN_NONPLAIN = 0.05;
-inline bool prefers_tma(const llb_lattice& h) {
-    return h.R * h.C >= TMA_MIN_NODES && h.n_active > 0 &&
-           static_cast<double>(h.n_nonplain) >= TMA_MIN_NONPLAIN * static_cast<double>(h.n_active);
+inline int default_pipeline(const llb_lattice& h) {
+    const int64_t n = h.R * h.C;
+    if (n < TMA_MIN_NODES || h.n_active == 0) return PIPE_GRID;
+    if (static_cast<double>(h.n_nonplain) >= TMA_MIN_NONPLAIN * static_cast<double>(h.n_active))
+        return h.storage == LLB_STORE_F64 && n >= (int64_t{1} << 21) ? 1 : 0;
+    const double state = 2.0 * 9.0 * static_cast<double>(h.elem) * static_cast<double>(n);
+    if (h.storage == LLB_STORE_F16S) return state >= static_cast<double>(int64_t{1} << 27) ? 0 : PIPE_GRID;
+    return state >= static_cast<double>(int64_t{1} << 28) ? llb::FIRST_PAIR_CONFIG : PIPE_GRID;
 }
 
 namespace llb {

@@ -1,5 +1,6 @@
 // Shifted low-precision kernels (populations stored as f - w in FP32 or FP16,
-// arithmetic in FP32).  Multiply-add contraction is allowed here.
+// arithmetic in FP32).  Compiled with --fmad=false: the model writes its
+// multiply-adds out, so every kernel of a form gives the same bits.
 #include "llb_kernel_inst.cuh"
 
 #include "../../include/llalbm_cuda.h"

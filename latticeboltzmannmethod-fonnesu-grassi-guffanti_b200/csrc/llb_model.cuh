@@ -5,7 +5,9 @@
 //              reference's association order (its translation unit is compiled
 //              with --fmad=false, so no multiply-add is contracted).
 //   ModelShift<T>  populations stored as f_k - w_k in T (float or __half);
-//              moments, closures and collision in FP32 on the shifted values.
+//              moments, closures and collision in FP32 on the shifted values,
+//              multiply-adds written out as __fmaf_rn (its translation unit is
+//              also compiled with --fmad=false).
 #pragma once
 
 #include "llb_internal.cuh"
@@ -203,26 +205,28 @@ struct ModelShift {
 
     static __device__ __forceinline__ void close(R* g, int side, R ru, R rv) {
         constexpr R two_thirds = 2.0f / 3.0f, one_sixth = 1.0f / 6.0f, one_half = 0.5f;
+        // multiply-adds written out (__fmaf_rn): the translation unit is built
+        // without automatic contraction, so every kernel rounds alike
         switch (side) {
         case SIDE_TOP:
-            g[4] = g[2] - two_thirds * rv;
-            g[7] = g[5] - one_sixth * rv - one_half * ru + one_half * (g[1] - g[3]);
-            g[8] = g[6] - one_sixth * rv + one_half * ru - one_half * (g[1] - g[3]);
+            g[4] = __fmaf_rn(-two_thirds, rv, g[2]);
+            g[7] = __fmaf_rn(one_half, g[1] - g[3], __fmaf_rn(-one_half, ru, __fmaf_rn(-one_sixth, rv, g[5])));
+            g[8] = __fmaf_rn(-one_half, g[1] - g[3], __fmaf_rn(one_half, ru, __fmaf_rn(-one_sixth, rv, g[6])));
             break;
         case SIDE_BOTTOM:
-            g[2] = g[4] + two_thirds * rv;
-            g[5] = g[7] + one_sixth * rv + one_half * ru - one_half * (g[1] - g[3]);
-            g[6] = g[8] + one_sixth * rv - one_half * ru + one_half * (g[1] - g[3]);
+            g[2] = __fmaf_rn(two_thirds, rv, g[4]);
+            g[5] = __fmaf_rn(-one_half, g[1] - g[3], __fmaf_rn(one_half, ru, __fmaf_rn(one_sixth, rv, g[7])));
+            g[6] = __fmaf_rn(one_half, g[1] - g[3], __fmaf_rn(-one_half, ru, __fmaf_rn(one_sixth, rv, g[8])));
             break;
         case SIDE_LEFT:
-            g[1] = g[3] + two_thirds * ru;
-            g[5] = g[7] + one_sixth * ru + one_half * rv - one_half * (g[2] - g[4]);
-            g[8] = g[6] + one_sixth * ru - one_half * rv + one_half * (g[2] - g[4]);
+            g[1] = __fmaf_rn(two_thirds, ru, g[3]);
+            g[5] = __fmaf_rn(-one_half, g[2] - g[4], __fmaf_rn(one_half, rv, __fmaf_rn(one_sixth, ru, g[7])));
+            g[8] = __fmaf_rn(one_half, g[2] - g[4], __fmaf_rn(-one_half, rv, __fmaf_rn(one_sixth, ru, g[6])));
             break;
         case SIDE_RIGHT:
-            g[3] = g[1] - two_thirds * ru;
-            g[7] = g[5] - one_sixth * ru - one_half * rv + one_half * (g[2] - g[4]);
-            g[6] = g[8] - one_sixth * ru + one_half * rv - one_half * (g[2] - g[4]);
+            g[3] = __fmaf_rn(-two_thirds, ru, g[1]);
+            g[7] = __fmaf_rn(one_half, g[2] - g[4], __fmaf_rn(-one_half, rv, __fmaf_rn(-one_sixth, ru, g[5])));
+            g[6] = __fmaf_rn(-one_half, g[2] - g[4], __fmaf_rn(one_half, rv, __fmaf_rn(-one_sixth, ru, g[8])));
             break;
         default:
             break;
@@ -232,10 +236,10 @@ struct ModelShift {
     // sum of the known populations' shifted values as the Zou-He density uses them
     static __device__ __forceinline__ R known_sum(const R* g, int side) {
         switch (side) {
-        case SIDE_TOP: return (g[0] + g[1] + g[3]) + 2.0f * (g[2] + g[5] + g[6]);
-        case SIDE_BOTTOM: return (g[0] + g[1] + g[3]) + 2.0f * (g[4] + g[7] + g[8]);
-        case SIDE_LEFT: return (g[0] + g[2] + g[4]) + 2.0f * (g[3] + g[7] + g[6]);
-        case SIDE_RIGHT: return (g[0] + g[2] + g[4]) + 2.0f * (g[1] + g[5] + g[8]);
+        case SIDE_TOP: return __fmaf_rn(2.0f, g[2] + g[5] + g[6], g[0] + g[1] + g[3]);
+        case SIDE_BOTTOM: return __fmaf_rn(2.0f, g[4] + g[7] + g[8], g[0] + g[1] + g[3]);
+        case SIDE_LEFT: return __fmaf_rn(2.0f, g[3] + g[7] + g[6], g[0] + g[2] + g[4]);
+        case SIDE_RIGHT: return __fmaf_rn(2.0f, g[1] + g[5] + g[8], g[0] + g[2] + g[4]);
         default: return 0.0f;
         }
     }
@@ -271,40 +275,43 @@ struct ModelShift {
     // of cu, so each pair is computed once: g_eq = w (even +- odd).
     template <int COLL>
     static __device__ __forceinline__ void collide(R* g, R drho, R ux, R uy, const Collision& c) {
+        // multiply-adds written out (__fmaf_rn): the translation unit is built
+        // without automatic contraction, so every kernel rounds alike
         const R rho = 1.0f + drho;
-        const R u2 = 1.5f * (ux * ux + uy * uy);
-        const R e0 = w_f32(0) * (drho - rho * u2);
+        const R u2 = 1.5f * __fmaf_rn(ux, ux, uy * uy);
+        const R e0 = w_f32(0) * __fmaf_rn(-rho, u2, drho);
         // pairs (1,3), (2,4), (5,7), (6,8): cu of the first direction of each pair
+        // (DJ, DI are 0 or +-1, so cu is a sum or difference of ux and uy)
         constexpr int first[4] = {1, 2, 5, 6};
         R ev[4], od[4];
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
             const int k = first[p];
             const R cu = static_cast<R>(DJ(k)) * ux - static_cast<R>(DI(k)) * uy;
-            ev[p] = w_f32(k) * (drho + rho * (4.5f * cu * cu - u2));
+            ev[p] = w_f32(k) * __fmaf_rn(rho, __fmaf_rn(4.5f * cu, cu, -u2), drho);
             od[p] = w_f32(k) * (rho * (3.0f * cu));
         }
         if (COLL == 0) {
             const R t = c.tf, omt = c.omtf;
-            g[0] = omt * g[0] + t * e0;
+            g[0] = __fmaf_rn(omt, g[0], t * e0);
 #pragma unroll
             for (int p = 0; p < 4; ++p) {
                 const int k = first[p], b = opp(k);
-                g[k] = omt * g[k] + t * (ev[p] + od[p]);
-                g[b] = omt * g[b] + t * (ev[p] - od[p]);
+                g[k] = __fmaf_rn(omt, g[k], t * (ev[p] + od[p]));
+                g[b] = __fmaf_rn(omt, g[b], t * (ev[p] - od[p]));
             }
         } else {
             const R ie = c.ief, he = c.hef, ho = c.hof;
-            g[0] = g[0] - ie * (g[0] - e0);
+            g[0] = __fmaf_rn(-ie, g[0] - e0, g[0]);
 #pragma unroll
             for (int p = 0; p < 4; ++p) {
                 const int k = first[p], b = opp(k);
                 // symmetric and antisymmetric non-equilibrium parts of the pair
-                const R sym = (g[k] + g[b]) - 2.0f * ev[p];
-                const R asym = (g[k] - g[b]) - 2.0f * od[p];
+                const R sym = __fmaf_rn(-2.0f, ev[p], g[k] + g[b]);
+                const R asym = __fmaf_rn(-2.0f, od[p], g[k] - g[b]);
                 const R qk = g[k], qb = g[b];
-                g[k] = qk - he * sym - ho * asym;
-                g[b] = qb - he * sym + ho * asym;
+                g[k] = __fmaf_rn(-ho, asym, __fmaf_rn(-he, sym, qk));
+                g[b] = __fmaf_rn(ho, asym, __fmaf_rn(-he, sym, qb));
             }
         }
     }

@@ -170,6 +170,21 @@ def test_shifted_storage_velocity_error(storage, tol, pipeline):
     assert err <= tol, err
 
 
+@pytest.mark.parametrize("storage", [1, 2], ids=["f32s", "f16s"])
+def test_shifted_forms_equal_across_kernels(storage):
+    """Shifted storage: every step kernel (list, grid, TMA, two steps per pass)
+    writes the same multiply-adds and keeps the two-step intermediate in the
+    storage type, so all of them give the same bits."""
+    lists = H.classify(H.porous_types(200, 300, fraction=0.25, rmin=2, rmax=6, seed=9))
+    p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.03:0", "pressure", 1)
+    outs = [run_gpu(lists, p, 101, table, storage=storage, pipeline=cfg) for cfg in (-1, -2, 0, 1, 2, 3, 4, 5)]
+    act = H.active_mask(lists)
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o["post"][:, act], outs[0]["post"][:, act])
+        np.testing.assert_array_equal(o["u"], outs[0]["u"])
+
+
 def test_flow_forces_and_gather():
     lists = H.classify(H.channel_types(48, 96, discs=[(24, 30, 6)]))
     p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
