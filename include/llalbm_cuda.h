@@ -369,6 +369,14 @@ int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, flo
    multiply-adds differently. */
 int llb_set_pipeline(llb_handle h, int32_t config);
 int llb_get_pipeline(llb_handle h, int32_t* config);
+/* Autotuner of one lattice (no reference counterpart): runs every plain-step
+   configuration this lattice supports (-1, -2, 0..5) for trial_steps warm-up
+   and trial_steps timed steps and keeps the fastest.  Every configuration
+   gives the same bits, so these are ordinary steps of the simulation: the
+   lattice advances by 2 x trial_steps per configuration tried (llb_get_step
+   tells how far), and their boundary values must be set as for llb_step.
+   best and ms_per_step (either may be NULL) receive the choice and its time. */
+int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* ms_per_step);
 /* Columns of lattice nodes per thread block of the one-thread-per-node kernel
    (1..8; each block is 32 rows x block_y columns). */
 int llb_set_launch_shape(llb_handle h, int32_t block_y);

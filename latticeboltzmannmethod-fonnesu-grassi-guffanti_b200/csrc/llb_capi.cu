@@ -852,6 +852,71 @@ int llb_get_pipeline(llb_handle h, int32_t* config) {
     return LLB_OK;
 }
 
+// Device buffers of the active-sector list, released when the tuner does not
+// keep the list kernel.
+static void release_sector_list(llb_handle h) {
+    const int64_t SN = LIST_BYTES / static_cast<int64_t>(h->elem);
+    if (h->d_sectors) {
+        cudaFree(h->d_sectors);
+        cudaFree(h->d_smask);
+        cudaFree(h->d_sbb);
+        h->bytes -= static_cast<int64_t>(h->n_sectors) * (static_cast<int64_t>(sizeof(int32_t)) + 2 * SN);
+    }
+    h->d_sectors = nullptr;
+    h->d_smask = nullptr;
+    h->d_sbb = nullptr;
+    h->n_sectors = 0;
+}
+
+int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* ms_per_step) {
+    if (!h || trial_steps < 2 || trial_steps > (1 << 20)) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->initialized) return fail(h, LLB_E_STATE, "llb_tune_pipeline before llb_init");
+    int rc = select_device(h);
+    if (rc) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    LLB_CUDA(h, cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(h, ce, "cudaEventCreate");
+    }
+    const int original = h->tma_cfg;
+    int chosen = original;
+    float chosen_ms = -1.0f;
+    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, 0, 1, 2, 3, 4, 5};
+    for (int cfg : kCandidates) {
+        if (llb_set_pipeline(h, cfg) != LLB_OK) continue;  // not available for this lattice
+        // warm-up (tensor maps, graphs), then the timed steps
+        if ((rc = llb_step(h, trial_steps, 0))) break;
+        cudaError_t te = cudaEventRecord(e0, h->stream);
+        if (te != cudaSuccess) {
+            rc = cuda_fail(h, te, "cudaEventRecord");
+            break;
+        }
+        if ((rc = llb_step(h, trial_steps, 0))) break;
+        float ms = 0.0f;
+        te = cudaEventRecord(e1, h->stream);
+        if (te == cudaSuccess) te = cudaEventSynchronize(e1);
+        if (te == cudaSuccess) te = cudaEventElapsedTime(&ms, e0, e1);
+        if (te != cudaSuccess) {
+            rc = cuda_fail(h, te, "timing a pipeline configuration");
+            break;
+        }
+        if (chosen_ms < 0.0f || ms < chosen_ms) {
+            chosen_ms = ms;
+            chosen = cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if ((rc = llb_set_pipeline(h, chosen))) return rc;
+    if (chosen != PIPE_LIST) release_sector_list(h);
+    if (best) *best = chosen;
+    if (ms_per_step) *ms_per_step = chosen_ms < 0.0f ? 0.0f : chosen_ms / static_cast<float>(trial_steps);
+    return LLB_OK;
+}
+
 int llb_set_launch_shape(llb_handle h, int32_t block_y) {
     if (!h || block_y < 1 || block_y > MAX_BLOCK_Y) return fail(h, LLB_E_INVALID, "block_y must be in [1, 8]");
     if (block_y != h->block_y) {

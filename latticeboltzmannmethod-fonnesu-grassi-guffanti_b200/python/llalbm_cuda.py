@@ -99,6 +99,7 @@ SIGNATURES = {
     "llb_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
     "llb_set_pipeline": [_H, ctypes.c_int32],
     "llb_get_pipeline": [_H, ctypes.POINTER(ctypes.c_int32)],
+    "llb_tune_pipeline": [_H, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
     "llb_set_launch_shape": [_H, ctypes.c_int32],
     "llb_compute_macro": [_H, _P, _P],
     "llb_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_H)],
@@ -368,6 +369,13 @@ class CudaLattice:
         c = ctypes.c_int32()
         _check(lib().llb_get_pipeline(self._h, ctypes.byref(c)), self._h)
         return c.value
+
+    def tune_pipeline(self, trial_steps: int = 32):
+        """Runs every plain-step configuration for 2 x trial_steps real steps
+        and keeps the fastest; returns (configuration, ms per step)."""
+        cfg, ms = ctypes.c_int32(), ctypes.c_float()
+        _check(lib().llb_tune_pipeline(self._h, trial_steps, ctypes.byref(cfg), ctypes.byref(ms)), self._h)
+        return cfg.value, ms.value
 
     def set_launch_shape(self, block_y: int):
         _check(lib().llb_set_launch_shape(self._h, block_y), self._h)

@@ -185,6 +185,30 @@ def test_shifted_forms_equal_across_kernels(storage):
         np.testing.assert_array_equal(o["u"], outs[0]["u"])
 
 
+@pytest.mark.parametrize("storage", [0, 1])
+def test_tune_pipeline_steps_are_ordinary_steps(storage):
+    """The autotuner runs real steps under every configuration it tries and
+    keeps the fastest; the lattice then holds exactly the state of that many
+    ordinary steps (FP64: the oracle's bits; FP32: a run without tuning)."""
+    lists = H.classify(H.porous_types(300, 400, seed=11))
+    p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.02:0", "pressure", 1)
+    with make_gpu(lists, p, storage=storage) as g:
+        g.set_open_values(pressure_table(table, lists, p), 0)
+        g.init()
+        cfg, ms = g.tune_pipeline(8)
+        assert cfg in (-2, -1, 0, 1, 2, 3, 4, 5) and ms > 0.0 and g.pipeline == cfg
+        assert g.t == 1 + 2 * 8 * 8  # init + warm-up and timed steps of all 8 configurations
+        g.step(5, macro=True)
+        steps = g.t
+        got_pop, (got_rho, got_u) = g.post_collision(), g.macro()
+    ref = H.run_oracle(lists, p, steps, table) if storage == 0 else run_gpu(lists, p, steps, table, storage=storage)
+    act = H.active_mask(lists)
+    np.testing.assert_array_equal(got_pop[:, act], ref["post"][:, act])
+    np.testing.assert_array_equal(got_u, ref["u"])
+    np.testing.assert_array_equal(got_rho, ref["rho"])
+
+
 def test_flow_forces_and_gather():
     lists = H.classify(H.channel_types(48, 96, discs=[(24, 30, 6)]))
     p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
