@@ -270,10 +270,14 @@ def oracle_cpu(wl: dict, types: np.ndarray, steps: int) -> dict:
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def bytes_per_step(storage_bytes: int, n_active: int, n_nodes: int) -> int:
+def bytes_per_step(storage_bytes: int, n_active: int, n_nodes: int, steps_per_pass: int = 1) -> int:
     """Algorithmic HBM bytes of one step: 9 populations read and 9 written per
-    active node, plus the 1-byte node mask of every node."""
-    return 18 * storage_bytes * n_active + n_nodes
+    active node, plus the 1-byte node mask of every node, once per pass over
+    the lattice (a two-steps-per-pass kernel moves them once for two steps)."""
+    return (18 * storage_bytes * n_active + n_nodes) // steps_per_pass
+
+
+PAIR_CONFIGS = (3, 4, 5)  # pipeline configurations that advance two steps per pass
 
 
 def make_lattice(L, wl, nodes, R, C, storage, device):
@@ -358,9 +362,10 @@ def run_ours(a, dist):
         g, ms, (t0, t1), u = time_form(L, wl, nodes, R, C, storage, dev, a.warmup, a.steps, dist, a.pipeline,
                                        a.launch_shape)
         per = ms / a.steps
-        bps = bytes_per_step(sb, n_active, R * C)
+        spp = 2 if g.pipeline in PAIR_CONFIGS else 1
+        bps = bytes_per_step(sb, n_active, R * C, spp)
         form = {"mlups": dist.world * R * C / per / 1e3, "ms_per_step": per, "gb_s": bps / per / 1e6,
-                "bytes_per_step": bps}
+                "bytes_per_step": bps, "pipeline": g.pipeline, "steps_per_pass": spp}
         if storage == 0:
             u_ref = u
             head = (g, ms, t0, t1)
@@ -423,7 +428,8 @@ def run_ours(a, dist):
         "roofline": {"bound": "hbm", "achieved": round(f64["gb_s"], 1), "peak": peak, "unit": "GB/s",
                      "frac": round(f64["gb_s"] / peak, 4), "traffic": traffic,
                      "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
-                     "algorithmic_bytes_per_launch": f64["bytes_per_step"]},
+                     "algorithmic_bytes_per_launch": f64["bytes_per_step"] * f64["steps_per_pass"],
+                     "steps_per_launch": f64["steps_per_pass"]},
         "forms": {k: {kk: (round(vv, 6) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                   for k, v in forms.items()},
         "e2e": {"value": round(dist.world * R * C * e2e_steps / e_s / 1e6, 1), "unit": "MLUPS",
