@@ -293,7 +293,7 @@ int launch_one(llb_handle h, bool macro, long long graph_offset = -1, bool singl
         if (!(h->plan.pair && single)) {
             const long long ntiles =
                 ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
-            const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
+            const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(h->sm_count) * h->plan.ctas_per_sm));
             cudaError_t e = launch_step_tma(h->storage, h->plan, x, &h->pmap[h->cur], &h->mmap, h->f[h->cur],
                                             h->f[h->cur ^ 1], grid);
             if (e != cudaSuccess) return cuda_fail(h, e, "pipelined step kernel launch");
@@ -408,7 +408,7 @@ int handle_launch_step(llb_handle h, int cur, const long long* tbase, long long 
         int rc = build_maps(h);
         if (rc) return rc;
         const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
-        const int grid = static_cast<int>(std::min<long long>(ntiles, h->sm_count));
+        const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(h->sm_count) * h->plan.ctas_per_sm));
         e = launch_step_tma(h->storage, h->plan, x, &h->pmap[cur], &h->mmap, h->f[cur], h->f[cur ^ 1], grid);
     } else {  // one step at a time in a batch: a two-step configuration uses the one-thread kernel
         e = launch_step(h->storage, x, h->f[cur], h->f[cur ^ 1], false, false);

@@ -32,7 +32,7 @@ using F64Cfg2 = TmaCfg<double, 128, 4, 4, 20>;
 // two steps per launch (tile rows, tile columns, stages, consumer warps)
 using F64Pair3 = PairCfg<double, 32, 16, 2, 16>;
 using F64Pair4 = PairCfg<double, 32, 16, 3, 16>;
-using F64Pair5 = PairCfg<double, 64, 8, 2, 16>;
+using F64Pair5 = PairCfg<double, 32, 16, 1, 8, 2>;
 
 bool tma_plan_f64(int cfg, TmaPlan* p) {
     switch (cfg) {

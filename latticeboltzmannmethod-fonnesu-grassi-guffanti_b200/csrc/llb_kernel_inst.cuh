@@ -98,6 +98,7 @@ template <class M, class CFG>
 void fill_plan(int cfg, TmaPlan* p) {
     p->cfg = cfg;
     p->pair = CFG::PAIR;
+    p->ctas_per_sm = CFG::CPS;
     p->TI = CFG::TI;
     p->TJ = CFG::TJ;
     p->S = CFG::S;
@@ -132,6 +133,9 @@ cudaError_t do_step_pair(const LaunchCtx& x, const CUtensorMap* pmap, const CUte
     auto k1 = k_step_pair<M, 1, CFG>;
     auto kern = x.c.model == 0 ? k0 : k1;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CFG::SMEM_BYTES);
+    // CFG::CPS CTAs of this kernel share an SM's shared memory
+    if (e == cudaSuccess && CFG::CPS > 1)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, x.g, x.ot, x.c, static_cast<const T*>(fin),
                                                              static_cast<T*>(fout), x.ss);

@@ -86,6 +86,7 @@ cudaError_t launch_gather_forces_lowp(int storage, const LaunchCtx&, const void*
 struct TmaPlan {
     int cfg = -1;
     bool pair = false;     // two steps per launch (k_step_pair)
+    int ctas_per_sm = 1;   // persistent grid = ctas_per_sm x SM count
     int TI = 0, TJ = 0, S = 0, W = 0;
     int BI = 0;            // rows of a population box
     int BJ = 0;            // columns of a population box

@@ -49,10 +49,10 @@ using F16Cfg2 = TmaCfg<__half, 128, 32, 2, 16>;
 // two steps per launch
 using F32Pair3 = PairCfg<float, 32, 32, 2, 16>;
 using F32Pair4 = PairCfg<float, 32, 32, 3, 16>;
-using F32Pair5 = PairCfg<float, 64, 16, 2, 16>;
+using F32Pair5 = PairCfg<float, 32, 32, 1, 8, 2>;
 using F16Pair3 = PairCfg<__half, 32, 64, 2, 16>;
 using F16Pair4 = PairCfg<__half, 64, 32, 2, 16>;
-using F16Pair5 = PairCfg<__half, 32, 32, 3, 16>;
+using F16Pair5 = PairCfg<__half, 32, 64, 1, 8, 2>;
 
 bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
     if (storage == LLB_STORE_F32S) {

@@ -36,9 +36,13 @@
 
 namespace llb {
 
-template <typename T, int TI_, int TJ_, int S_, int W_>
+// CPS: CTAs per SM (the persistent grid is CPS x the SM count).  Two CTAs
+// with one stage each let one CTA compute while the other waits for its tile
+// or at a phase barrier.
+template <typename T, int TI_, int TJ_, int S_, int W_, int CPS_ = 1>
 struct PairCfg {
     static constexpr bool PAIR = true;
+    static constexpr int CPS = CPS_;
     static constexpr int TI = TI_, TJ = TJ_, S = S_, W = W_;
     static constexpr int A = 16 / static_cast<int>(sizeof(T));     // elements per 16 bytes
     static constexpr int HA = A >= 2 ? A : 2;                       // box rows above the tile
@@ -56,7 +60,7 @@ struct PairCfg {
     static constexpr int SMEM_BYTES = S * STAGE_BYTES + MID_BYTES + 2 * S * 8 + 16;
     static constexpr int THREADS = 32 * (W + 1);
     static_assert(TI % 32 == 0 && BI <= 256 && BJ <= 256 && BIM <= 256 && BJM <= 256, "TMA box limits");
-    static_assert(SMEM_BYTES <= 232448, "shared memory per block");
+    static_assert(SMEM_BYTES <= 232448 && CPS * (SMEM_BYTES + 1024) <= 233472, "shared memory per SM");
 };
 
 __device__ __forceinline__ void consumer_barrier(int threads) {
@@ -64,7 +68,7 @@ __device__ __forceinline__ void consumer_barrier(int threads) {
 }
 
 template <class M, int COLL, class CFG>
-__global__ void __launch_bounds__(CFG::THREADS, 1)
+__global__ void __launch_bounds__(CFG::THREADS, CFG::CPS)
     k_step_pair(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap mmap, Geometry g,
                 OpenTable ot, Collision c, const typename M::T* __restrict__ fin, typename M::T* __restrict__ fout,
                 StepSync ss) {

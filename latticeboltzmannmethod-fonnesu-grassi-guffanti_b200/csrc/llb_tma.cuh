@@ -80,6 +80,7 @@ constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 template <typename T, int TI_, int TJ_, int S_, int W_>
 struct TmaCfg {
     static constexpr bool PAIR = false;
+    static constexpr int CPS = 1;  // CTAs per SM
     static constexpr int TI = TI_, TJ = TJ_, S = S_, W = W_;
     static constexpr int A = 16 / static_cast<int>(sizeof(T));  // rows per 16 bytes
     static constexpr int BI = TI + A;                           // rows of a population box
