@@ -636,6 +636,12 @@ class OutputWriter:
             if rc != LLB_OK:
                 raise LLBError(rc, "llb_writer_destroy")
 
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
     def __enter__(self):
         return self
 
