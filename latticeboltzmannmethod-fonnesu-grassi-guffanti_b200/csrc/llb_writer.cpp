@@ -202,27 +202,44 @@ void format_rows(const double* u, int64_t R, int64_t C, int64_t i0, int64_t i1, 
 }
 
 // Formats and writes one slot's two files; returns an error message or "".
+// Formats band t of T; false if its buffers could not be allocated.
+bool format_band(llb_writer* w, const Slot& s, int t, int T) noexcept {
+    try {
+        format_rows(s.buf, s.R, s.C, s.R * t / T, s.R * (t + 1) / T, w->bx[t], w->by[t], w->bt[t]);
+        return true;
+    } catch (...) {
+        return false;
+    }
+}
+
 std::string write_slot(llb_writer* w, const Slot& s) {
-    const int64_t R = s.R, C = s.C;
+    const int64_t R = s.R;
     const int T = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(w->nthreads, R)));
-    if (static_cast<int>(w->bx.size()) < T) {
-        w->bx.resize(T);
-        w->by.resize(T);
-        w->bt.resize(T);
+    try {
+        if (static_cast<int>(w->bx.size()) < T) {
+            w->bx.resize(T);
+            w->by.resize(T);
+            w->bt.resize(T);
+        }
+    } catch (...) {
+        return "host allocation of the formatting buffers failed";
     }
-    auto rows = [&](int t) { return std::make_pair(R * t / T, R * (t + 1) / T); };
+    // bands 1..T-1 on helper threads (a band whose thread cannot start runs here)
+    std::vector<char> ok(static_cast<size_t>(T), 0);
     std::vector<std::thread> pool;
-    pool.reserve(T - 1);
-    for (int t = 1; t < T; ++t)
-        pool.emplace_back([&, t] {
-            const auto [a, b] = rows(t);
-            format_rows(s.buf, R, C, a, b, w->bx[t], w->by[t], w->bt[t]);
-        });
-    {
-        const auto [a, b] = rows(0);
-        format_rows(s.buf, R, C, a, b, w->bx[0], w->by[0], w->bt[0]);
+    std::vector<int> inline_bands;
+    for (int t = 1; t < T; ++t) {
+        try {
+            pool.emplace_back([w, &s, &ok, t, T] { ok[static_cast<size_t>(t)] = format_band(w, s, t, T); });
+        } catch (...) {
+            inline_bands.push_back(t);
+        }
     }
+    ok[0] = format_band(w, s, 0, T);
+    for (int t : inline_bands) ok[static_cast<size_t>(t)] = format_band(w, s, t, T);
     for (auto& th : pool) th.join();
+    for (int t = 0; t < T; ++t)
+        if (!ok[static_cast<size_t>(t)]) return "host allocation of the formatting buffers failed";
     for (int d = 0; d < 2; ++d) {
         const std::string path = w->dir + "/output-" + std::to_string(s.index) + (d == 0 ? "u_x.txt" : "u_y.txt");
         std::FILE* f = std::fopen(path.c_str(), "wb");
@@ -340,7 +357,12 @@ int llb_writer_create(const char* dir, int32_t slots, int32_t threads, llb_write
     w->slots.resize(slots ? slots : 3);
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     w->nthreads = threads ? threads : static_cast<int>(std::min(16u, hw));
-    w->io = std::thread(io_loop, w);
+    try {
+        w->io = std::thread(io_loop, w);
+    } catch (...) {
+        delete w;
+        return LLB_E_NOMEM;
+    }
     *out = w;
     return LLB_OK;
 }
