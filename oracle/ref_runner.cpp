@@ -43,6 +43,7 @@ struct Options {
     double rho_out = 1.0, tangential_u = 0.0;
     std::string obstacle = "bb";    // bb | ps (PSBounceBackPolicy, serial policies)
     double ps_tau = 0.6;
+    std::string ps_b = "default";   // default | pattern (b of obstacle q = ((37 q + 11) mod 101) / 100)
     long steps = 10;
     long warmup = 0;
     long analyzer_every = 0;
@@ -332,6 +333,15 @@ int run_case(const Options& o) {
         // compute_obstacle_weight fills copies of the nodes, so every b stays 1
         S::Obst::initialize(o.ps_tau);
         lat->compute_obstacle_weight();
+        if (o.ps_b == "pattern") {
+            // per-obstacle weights set on the lattice's own nodes (ObstaclePoint::set_b),
+            // which the policy reads (PSBounceBackPolicy.hpp:193)
+            auto& obs = lat->get_obstacle_nodes();
+            for (std::size_t q = 0; q < obs.size(); ++q)
+                obs[q].set_b(static_cast<double>((37 * q + 11) % 101) / 100.0);
+        } else if (o.ps_b != "default") {
+            die("bad --ps-b");
+        }
     }
     boundaries::ZouHePressurePolicy<2>::initialize(o.rho_out, o.tangential_u);
     boundaries::ZouHePressurePolicy<2>::reset();
@@ -424,6 +434,7 @@ int main(int argc, char** argv) {
         else if (k == "--tangential-u") o.tangential_u = std::stod(val());
         else if (k == "--obstacle") o.obstacle = val();
         else if (k == "--ps-tau") o.ps_tau = std::stod(val());
+        else if (k == "--ps-b") o.ps_b = val();
         else if (k == "--steps") o.steps = std::stol(val());
         else if (k == "--warmup") o.warmup = std::stol(val());
         else if (k == "--analyzer") o.analyzer_every = std::stol(val());

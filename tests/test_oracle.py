@@ -110,6 +110,8 @@ def ref_vs_oracle(types, args, steps, tmp_path, extra=()):
     lists = H.ref_lists(res)
     assert_lists_equal(lists, H.classify(types))
     p, ins, outs = params_from_args(args)
+    if "--ps-b" in args:  # the runner's per-obstacle weight pattern
+        p.obstacle_b = np.array([((37 * q + 11) % 101) / 100.0 for q in range(len(lists.obstacle))])
     table = H.open_values(lists, ins, outs, steps)
     got = H.run_oracle(lists, p, steps, table)
     R, C = lists.rows, lists.cols
@@ -163,3 +165,14 @@ def test_live_reference_partially_saturated_obstacles(coll, tmp_path):
     cav[((ii - 24) ** 2 + (jj - 24) ** 2 <= 64) & (cav == H.FLUID)] = H.OBSTACLE
     ref_vs_oracle(cav, col + ["--obstacle", "ps", "--ps-tau", "0.51", "--inlet", "zh", "--outlet", "zh",
                               "--inlet-u", "lidramp:0.1:0.002"], 200, tmp_path / "cav")
+
+
+@needs_ref
+def test_live_reference_partially_saturated_per_obstacle_b(tmp_path):
+    """PSBounceBackPolicy with a weight b in [0, 1] set on each obstacle node
+    (ObstaclePoint::set_b) before the run: the oracle's per-obstacle b path
+    equals the reference bit for bit."""
+    ch = H.channel_types(40, 90, discs=[(20, 30, 7), (12, 62, 4)])
+    ref_vs_oracle(ch, ["--collision", "trt", "--tau-even", "0.6", "--magic", "0.25", "--obstacle", "ps",
+                       "--ps-tau", "0.7", "--ps-b", "pattern", "--inlet", "zh", "--outlet", "zhp",
+                       "--inlet-u", "parabolic:0.04:1:38", "--outlet-u", "pressure"], 150, tmp_path / "ch")
