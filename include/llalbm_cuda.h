@@ -357,7 +357,8 @@ int llb_check_numerics(llb_handle h);
 int llb_event_record(llb_handle h, int32_t slot);
 int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, float* ms);
 /* Step-kernel selection, for the autotuner.  Plain steps run the TMA-pipelined
-   kernel in configuration `config` (0..2: tile shape, stage count, warps), the
+   kernel in configuration `config` (0..2: tile shape, stage count, warps; 6:
+   the form's default shape with the tile's bounce bytes loaded too), the
    two-steps-per-pass kernel (3..5: the intermediate step stays in shared
    memory, so a pair of steps reads and writes the populations once; a lone
    step runs on the one-thread kernel), the one-thread-per-node kernel for
@@ -370,7 +371,7 @@ int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, flo
 int llb_set_pipeline(llb_handle h, int32_t config);
 int llb_get_pipeline(llb_handle h, int32_t* config);
 /* Autotuner of one lattice (no reference counterpart): runs every plain-step
-   configuration this lattice supports (-1, -2, 0..5) for trial_steps warm-up
+   configuration this lattice supports (-1, -2, 0..6) for trial_steps warm-up
    and trial_steps timed steps and keeps the fastest.  Every configuration
    gives the same bits, so these are ordinary steps of the simulation: the
    lattice advances by 2 x trial_steps per configuration tried (llb_get_step

@@ -268,6 +268,16 @@ int build_maps(llb_handle h) {
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(h, LLB_E_CUDA, "cuTensorMapEncodeTiled (mask) failed");
+    // bounce bytes, (ld, C) bytes with boxes of TI x TJ (a copy of the mask map
+    // when the configuration does not load them: the kernel never reads it)
+    h->bmap = h->mmap;
+    if (h->plan.bbx) {
+        const cuuint32_t bbox[2] = {static_cast<cuuint32_t>(h->plan.TI), static_cast<cuuint32_t>(h->plan.TJ)};
+        r = enc(&h->bmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, h->d_bb, mdims, mstrides, bbox, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(h, LLB_E_CUDA, "cuTensorMapEncodeTiled (bounce bytes) failed");
+    }
     h->maps_ready = true;
     return LLB_OK;
 }
@@ -294,8 +304,8 @@ int launch_one(llb_handle h, bool macro, long long graph_offset = -1, bool singl
             const long long ntiles =
                 ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
             const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(h->sm_count) * h->plan.ctas_per_sm));
-            cudaError_t e = launch_step_tma(h->storage, h->plan, x, &h->pmap[h->cur], &h->mmap, h->f[h->cur],
-                                            h->f[h->cur ^ 1], grid);
+            cudaError_t e = launch_step_tma(h->storage, h->plan, x, &h->pmap[h->cur], &h->mmap, &h->bmap,
+                                            h->f[h->cur], h->f[h->cur ^ 1], grid);
             if (e != cudaSuccess) return cuda_fail(h, e, "pipelined step kernel launch");
             h->cur ^= 1;
             h->step += h->plan.pair ? 2 : 1;
@@ -370,9 +380,9 @@ bool tma_plan(int s, int cfg, TmaPlan* out) {
     return s == LLB_STORE_F64 ? tma_plan_f64(cfg, out) : tma_plan_lowp(s, cfg, out);
 }
 cudaError_t launch_step_tma(int s, const TmaPlan& p, const LaunchCtx& x, const CUtensorMap* pm, const CUtensorMap* mm,
-                            const void* fin, void* fout, int grid) {
-    return s == LLB_STORE_F64 ? launch_step_tma_f64(p, x, pm, mm, fin, fout, grid)
-                              : launch_step_tma_lowp(s, p, x, pm, mm, fin, fout, grid);
+                            const CUtensorMap* bm, const void* fin, void* fout, int grid) {
+    return s == LLB_STORE_F64 ? launch_step_tma_f64(p, x, pm, mm, bm, fin, fout, grid)
+                              : launch_step_tma_lowp(s, p, x, pm, mm, bm, fin, fout, grid);
 }
 cudaError_t launch_gather_forces(int s, const LaunchCtx& x, const void* fin, const int64_t* pts, const uint16_t* dirs,
                                  long long n, double* out) {
@@ -409,7 +419,8 @@ int handle_launch_step(llb_handle h, int cur, const long long* tbase, long long 
         if (rc) return rc;
         const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
         const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(h->sm_count) * h->plan.ctas_per_sm));
-        e = launch_step_tma(h->storage, h->plan, x, &h->pmap[cur], &h->mmap, h->f[cur], h->f[cur ^ 1], grid);
+        e = launch_step_tma(h->storage, h->plan, x, &h->pmap[cur], &h->mmap, &h->bmap, h->f[cur], h->f[cur ^ 1],
+                            grid);
     } else {  // one step at a time in a batch: a two-step configuration uses the one-thread kernel
         e = launch_step(h->storage, x, h->f[cur], h->f[cur ^ 1], false, false);
     }
@@ -830,7 +841,7 @@ static int build_sector_list(llb_handle h) {
 
 int llb_set_pipeline(llb_handle h, int32_t config) {
     if (!h || config < PIPE_LIST || config >= TMA_CONFIGS)
-        return fail(h, LLB_E_INVALID, "config must be -2, -1 or in [0, 6)");
+        return fail(h, LLB_E_INVALID, "config must be -2, -1 or in [0, 7)");
     if (config != PIPE_GRID && h->d_ps)
         return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
     if (config != h->tma_cfg) {
@@ -883,7 +894,7 @@ int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* m
     const int original = h->tma_cfg;
     int chosen = original;
     float chosen_ms = -1.0f;
-    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, 0, 1, 2, 3, 4, 5};
+    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, 0, 1, 2, 3, 4, 5, 6};
     for (int cfg : kCandidates) {
         if (llb_set_pipeline(h, cfg) != LLB_OK) continue;  // not available for this lattice
         // warm-up (tensor maps, graphs), then the timed steps

@@ -33,6 +33,8 @@ using F64Cfg2 = TmaCfg<double, 128, 4, 4, 20>;
 using F64Pair3 = PairCfg<double, 32, 16, 2, 16>;
 using F64Pair4 = PairCfg<double, 32, 16, 3, 16>;
 using F64Pair5 = PairCfg<double, 32, 16, 1, 8, 2>;
+// configuration 1 with the tile's bounce bytes
+using F64Cfg6 = TmaCfg<double, 128, 8, 2, 16, true>;
 
 bool tma_plan_f64(int cfg, TmaPlan* p) {
     switch (cfg) {
@@ -42,19 +44,21 @@ bool tma_plan_f64(int cfg, TmaPlan* p) {
     case 3: fill_plan<ModelF64, F64Pair3>(3, p); return true;
     case 4: fill_plan<ModelF64, F64Pair4>(4, p); return true;
     case 5: fill_plan<ModelF64, F64Pair5>(5, p); return true;
+    case 6: fill_plan<ModelF64, F64Cfg6>(6, p); return true;
     default: return false;
     }
 }
 
 cudaError_t launch_step_tma_f64(const TmaPlan& p, const LaunchCtx& x, const CUtensorMap* pm, const CUtensorMap* mm,
-                                const void* fin, void* fout, int grid) {
+                                const CUtensorMap* bm, const void* fin, void* fout, int grid) {
     switch (p.cfg) {
-    case 0: return do_step_tma<ModelF64, F64Cfg0>(x, pm, mm, fin, fout, grid);
-    case 1: return do_step_tma<ModelF64, F64Cfg1>(x, pm, mm, fin, fout, grid);
-    case 2: return do_step_tma<ModelF64, F64Cfg2>(x, pm, mm, fin, fout, grid);
-    case 3: return do_step_pair<ModelF64, F64Pair3>(x, pm, mm, fin, fout, grid);
-    case 4: return do_step_pair<ModelF64, F64Pair4>(x, pm, mm, fin, fout, grid);
-    case 5: return do_step_pair<ModelF64, F64Pair5>(x, pm, mm, fin, fout, grid);
+    case 0: return do_step_tma<ModelF64, F64Cfg0>(x, pm, mm, bm, fin, fout, grid);
+    case 1: return do_step_tma<ModelF64, F64Cfg1>(x, pm, mm, bm, fin, fout, grid);
+    case 2: return do_step_tma<ModelF64, F64Cfg2>(x, pm, mm, bm, fin, fout, grid);
+    case 3: return do_step_pair<ModelF64, F64Pair3>(x, pm, mm, bm, fin, fout, grid);
+    case 4: return do_step_pair<ModelF64, F64Pair4>(x, pm, mm, bm, fin, fout, grid);
+    case 5: return do_step_pair<ModelF64, F64Pair5>(x, pm, mm, bm, fin, fout, grid);
+    case 6: return do_step_tma<ModelF64, F64Cfg6>(x, pm, mm, bm, fin, fout, grid);
     default: return cudaErrorInvalidValue;
     }
 }

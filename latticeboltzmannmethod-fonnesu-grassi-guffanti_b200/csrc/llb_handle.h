@@ -65,6 +65,7 @@ struct llb_lattice {
     bool maps_ready = false;
     CUtensorMap pmap[2];  // populations f[0], f[1]
     CUtensorMap mmap;     // node mask
+    CUtensorMap bmap;     // bounce bytes (configurations that load them)
     int sm_count = 148;
     // active nodes with a wall, obstacle, dead or outside source (not PLAIN)
     int64_t n_active = 0, n_nonplain = 0;
@@ -76,8 +77,9 @@ struct llb_lattice {
 //  * below 2^19 nodes: one thread per node;
 //  * at least 5 % of the active nodes not PLAIN (porous media): the TMA
 //    pipeline -- FP64 configuration 1 from 2^21 nodes, else 0; configuration
-//    0 for the shifted forms (its bounce-back is a shared-memory address
-//    select, and its tiles stage every node);
+//    6 for the shifted forms (configuration 0 plus the tile's bounce bytes);
+//    its bounce-back is a shared-memory address select, and its tiles stage
+//    every node;
 //  * open flow whose resident state (two buffers of 9 planes) exceeds the L2
 //    cache several times over: two steps per pass for FP64 and FP32
 //    (configuration 3, from 2^28 bytes), the TMA pipeline for FP16 (from 2^27
@@ -91,7 +93,7 @@ inline int default_pipeline(const llb_lattice& h) {
     const int64_t n = h.R * h.C;
     if (n < TMA_MIN_NODES || h.n_active == 0) return PIPE_GRID;
     if (static_cast<double>(h.n_nonplain) >= TMA_MIN_NONPLAIN * static_cast<double>(h.n_active))
-        return h.storage == LLB_STORE_F64 && n >= (int64_t{1} << 21) ? 1 : 0;
+        return h.storage == LLB_STORE_F64 ? (n >= (int64_t{1} << 21) ? 1 : 0) : 6;
     const double state = 2.0 * 9.0 * static_cast<double>(h.elem) * static_cast<double>(n);
     if (h.storage == LLB_STORE_F16S) return state >= static_cast<double>(int64_t{1} << 27) ? 0 : PIPE_GRID;
     return state >= static_cast<double>(int64_t{1} << 28) ? llb::FIRST_PAIR_CONFIG : PIPE_GRID;

@@ -99,6 +99,7 @@ void fill_plan(int cfg, TmaPlan* p) {
     p->cfg = cfg;
     p->pair = CFG::PAIR;
     p->ctas_per_sm = CFG::CPS;
+    if constexpr (!CFG::PAIR) p->bbx = CFG::BBX;
     p->TI = CFG::TI;
     p->TJ = CFG::TJ;
     p->S = CFG::S;
@@ -112,22 +113,22 @@ void fill_plan(int cfg, TmaPlan* p) {
 }
 
 template <class M, class CFG>
-cudaError_t do_step_tma(const LaunchCtx& x, const CUtensorMap* pmap, const CUtensorMap* mmap, const void* fin,
-                        void* fout, int grid) {
+cudaError_t do_step_tma(const LaunchCtx& x, const CUtensorMap* pmap, const CUtensorMap* mmap,
+                        const CUtensorMap* bmap, const void* fin, void* fout, int grid) {
     using T = typename M::T;
     auto k0 = k_step_tma<M, 0, CFG>;
     auto k1 = k_step_tma<M, 1, CFG>;
     auto kern = x.c.model == 0 ? k0 : k1;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CFG::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, x.g, x.ot, x.c, static_cast<const T*>(fin),
-                                                             static_cast<T*>(fout), x.ss);
+    kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, *bmap, x.g, x.ot, x.c,
+                                                             static_cast<const T*>(fin), static_cast<T*>(fout), x.ss);
     return cudaGetLastError();
 }
 
 template <class M, class CFG>
-cudaError_t do_step_pair(const LaunchCtx& x, const CUtensorMap* pmap, const CUtensorMap* mmap, const void* fin,
-                         void* fout, int grid) {
+cudaError_t do_step_pair(const LaunchCtx& x, const CUtensorMap* pmap, const CUtensorMap* mmap,
+                         const CUtensorMap* bmap, const void* fin, void* fout, int grid) {
     using T = typename M::T;
     auto k0 = k_step_pair<M, 0, CFG>;
     auto k1 = k_step_pair<M, 1, CFG>;
@@ -137,8 +138,8 @@ cudaError_t do_step_pair(const LaunchCtx& x, const CUtensorMap* pmap, const CUte
     if (e == cudaSuccess && CFG::CPS > 1)
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, x.g, x.ot, x.c, static_cast<const T*>(fin),
-                                                             static_cast<T*>(fout), x.ss);
+    kern<<<grid, CFG::THREADS, CFG::SMEM_BYTES, x.stream>>>(*pmap, *mmap, *bmap, x.g, x.ot, x.c,
+                                                             static_cast<const T*>(fin), static_cast<T*>(fout), x.ss);
     return cudaGetLastError();
 }
 

@@ -87,6 +87,7 @@ struct TmaPlan {
     int cfg = -1;
     bool pair = false;     // two steps per launch (k_step_pair)
     int ctas_per_sm = 1;   // persistent grid = ctas_per_sm x SM count
+    bool bbx = false;      // the producer also loads a TI x TJ box of bounce bytes
     int TI = 0, TJ = 0, S = 0, W = 0;
     int BI = 0;            // rows of a population box
     int BJ = 0;            // columns of a population box
@@ -95,19 +96,19 @@ struct TmaPlan {
     int threads = 0;
 };
 // Configurations 0..2: one step per launch (k_step_tma); 3..5: two steps per
-// launch (k_step_pair).
-constexpr int TMA_CONFIGS = 6;
+// launch (k_step_pair); 6: one step per launch with the tile's bounce bytes.
+constexpr int TMA_CONFIGS = 7;
 constexpr int FIRST_PAIR_CONFIG = 3;
 // Fills `out` for configuration `cfg` (0..TMA_CONFIGS-1) of a storage form.
 bool tma_plan(int storage, int cfg, TmaPlan* out);
 cudaError_t launch_step_tma(int storage, const TmaPlan& p, const LaunchCtx& ctx, const CUtensorMap* pmap,
-                            const CUtensorMap* mmap, const void* fin, void* fout, int grid);
+                            const CUtensorMap* mmap, const CUtensorMap* bmap, const void* fin, void* fout, int grid);
 bool tma_plan_f64(int cfg, TmaPlan* out);
 cudaError_t launch_step_tma_f64(const TmaPlan&, const LaunchCtx&, const CUtensorMap*, const CUtensorMap*,
-                                const void*, void*, int);
+                                const CUtensorMap*, const void*, void*, int);
 bool tma_plan_lowp(int storage, int cfg, TmaPlan* out);
 cudaError_t launch_step_tma_lowp(int storage, const TmaPlan&, const LaunchCtx&, const CUtensorMap*,
-                                 const CUtensorMap*, const void*, void*, int);
+                                 const CUtensorMap*, const CUtensorMap*, const void*, void*, int);
 
 inline dim3 node_grid(const Geometry& g, int bx, int by) {
     return dim3(static_cast<unsigned>((g.rows + bx - 1) / bx), static_cast<unsigned>((g.cols + by - 1) / by));

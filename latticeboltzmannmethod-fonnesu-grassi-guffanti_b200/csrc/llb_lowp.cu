@@ -53,6 +53,9 @@ using F32Pair5 = PairCfg<float, 32, 32, 1, 8, 2>;
 using F16Pair3 = PairCfg<__half, 32, 64, 2, 16>;
 using F16Pair4 = PairCfg<__half, 64, 32, 2, 16>;
 using F16Pair5 = PairCfg<__half, 32, 64, 1, 8, 2>;
+// configuration 0 with the tile's bounce bytes
+using F32Cfg6 = TmaCfg<float, 128, 8, 3, 16, true>;
+using F16Cfg6 = TmaCfg<__half, 128, 24, 3, 24, true>;
 
 bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
     if (storage == LLB_STORE_F32S) {
@@ -63,6 +66,7 @@ bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
         case 3: fill_plan<ModelF32S, F32Pair3>(3, p); return true;
         case 4: fill_plan<ModelF32S, F32Pair4>(4, p); return true;
         case 5: fill_plan<ModelF32S, F32Pair5>(5, p); return true;
+        case 6: fill_plan<ModelF32S, F32Cfg6>(6, p); return true;
         default: return false;
         }
     }
@@ -73,30 +77,34 @@ bool tma_plan_lowp(int storage, int cfg, TmaPlan* p) {
     case 3: fill_plan<ModelF16S, F16Pair3>(3, p); return true;
     case 4: fill_plan<ModelF16S, F16Pair4>(4, p); return true;
     case 5: fill_plan<ModelF16S, F16Pair5>(5, p); return true;
+    case 6: fill_plan<ModelF16S, F16Cfg6>(6, p); return true;
     default: return false;
     }
 }
 
 cudaError_t launch_step_tma_lowp(int storage, const TmaPlan& p, const LaunchCtx& x, const CUtensorMap* pm,
-                                 const CUtensorMap* mm, const void* fin, void* fout, int grid) {
+                                 const CUtensorMap* mm, const CUtensorMap* bm, const void* fin, void* fout,
+                                 int grid) {
     if (storage == LLB_STORE_F32S) {
         switch (p.cfg) {
-        case 0: return do_step_tma<ModelF32S, F32Cfg0>(x, pm, mm, fin, fout, grid);
-        case 1: return do_step_tma<ModelF32S, F32Cfg1>(x, pm, mm, fin, fout, grid);
-        case 2: return do_step_tma<ModelF32S, F32Cfg2>(x, pm, mm, fin, fout, grid);
-        case 3: return do_step_pair<ModelF32S, F32Pair3>(x, pm, mm, fin, fout, grid);
-        case 4: return do_step_pair<ModelF32S, F32Pair4>(x, pm, mm, fin, fout, grid);
-        case 5: return do_step_pair<ModelF32S, F32Pair5>(x, pm, mm, fin, fout, grid);
+        case 0: return do_step_tma<ModelF32S, F32Cfg0>(x, pm, mm, bm, fin, fout, grid);
+        case 1: return do_step_tma<ModelF32S, F32Cfg1>(x, pm, mm, bm, fin, fout, grid);
+        case 2: return do_step_tma<ModelF32S, F32Cfg2>(x, pm, mm, bm, fin, fout, grid);
+        case 3: return do_step_pair<ModelF32S, F32Pair3>(x, pm, mm, bm, fin, fout, grid);
+        case 4: return do_step_pair<ModelF32S, F32Pair4>(x, pm, mm, bm, fin, fout, grid);
+        case 5: return do_step_pair<ModelF32S, F32Pair5>(x, pm, mm, bm, fin, fout, grid);
+        case 6: return do_step_tma<ModelF32S, F32Cfg6>(x, pm, mm, bm, fin, fout, grid);
         default: return cudaErrorInvalidValue;
         }
     }
     switch (p.cfg) {
-    case 0: return do_step_tma<ModelF16S, F16Cfg0>(x, pm, mm, fin, fout, grid);
-    case 1: return do_step_tma<ModelF16S, F16Cfg1>(x, pm, mm, fin, fout, grid);
-    case 2: return do_step_tma<ModelF16S, F16Cfg2>(x, pm, mm, fin, fout, grid);
-    case 3: return do_step_pair<ModelF16S, F16Pair3>(x, pm, mm, fin, fout, grid);
-    case 4: return do_step_pair<ModelF16S, F16Pair4>(x, pm, mm, fin, fout, grid);
-    case 5: return do_step_pair<ModelF16S, F16Pair5>(x, pm, mm, fin, fout, grid);
+    case 0: return do_step_tma<ModelF16S, F16Cfg0>(x, pm, mm, bm, fin, fout, grid);
+    case 1: return do_step_tma<ModelF16S, F16Cfg1>(x, pm, mm, bm, fin, fout, grid);
+    case 2: return do_step_tma<ModelF16S, F16Cfg2>(x, pm, mm, bm, fin, fout, grid);
+    case 3: return do_step_pair<ModelF16S, F16Pair3>(x, pm, mm, bm, fin, fout, grid);
+    case 4: return do_step_pair<ModelF16S, F16Pair4>(x, pm, mm, bm, fin, fout, grid);
+    case 5: return do_step_pair<ModelF16S, F16Pair5>(x, pm, mm, bm, fin, fout, grid);
+    case 6: return do_step_tma<ModelF16S, F16Cfg6>(x, pm, mm, bm, fin, fout, grid);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -69,7 +69,8 @@ __device__ __forceinline__ void consumer_barrier(int threads) {
 
 template <class M, int COLL, class CFG>
 __global__ void __launch_bounds__(CFG::THREADS, CFG::CPS)
-    k_step_pair(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap mmap, Geometry g,
+    k_step_pair(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap mmap,
+                const __grid_constant__ CUtensorMap, Geometry g,
                 OpenTable ot, Collision c, const typename M::T* __restrict__ fin, typename M::T* __restrict__ fout,
                 StepSync ss) {
     using T = typename M::T;

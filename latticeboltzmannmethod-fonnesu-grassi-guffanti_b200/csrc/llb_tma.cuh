@@ -77,9 +77,13 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
 // Compile-time layout of one pipeline configuration.
-template <typename T, int TI_, int TJ_, int S_, int W_>
+// BBX: the producer also brings the tile's bounce bytes (one byte per node,
+// bit k-1 set when direction k's source is a wall or wet obstacle), so a
+// non-PLAIN node tests one byte instead of its eight neighbours' masks.
+template <typename T, int TI_, int TJ_, int S_, int W_, bool BBX_ = false>
 struct TmaCfg {
     static constexpr bool PAIR = false;
+    static constexpr bool BBX = BBX_;
     static constexpr int CPS = 1;  // CTAs per SM
     static constexpr int TI = TI_, TJ = TJ_, S = S_, W = W_;
     static constexpr int A = 16 / static_cast<int>(sizeof(T));  // rows per 16 bytes
@@ -89,8 +93,10 @@ struct TmaCfg {
     static constexpr int BJM = TJ + 2;                          // columns of the mask box (y0 = j0 - 1)
     static constexpr int PLANE_BYTES = round128(BI * BJ * static_cast<int>(sizeof(T)));
     static constexpr int MASK_BYTES = round128(BIM * BJM);
-    static constexpr int STAGE_BYTES = 9 * PLANE_BYTES + MASK_BYTES;
-    static constexpr unsigned TX_BYTES = 9u * BI * BJ * sizeof(T) + static_cast<unsigned>(BIM * BJM);
+    static constexpr int BB_BYTES = BBX ? round128(TI * TJ) : 0;  // bounce-byte box (x0 = i0, y0 = j0)
+    static constexpr int STAGE_BYTES = 9 * PLANE_BYTES + MASK_BYTES + BB_BYTES;
+    static constexpr unsigned TX_BYTES =
+        9u * BI * BJ * sizeof(T) + static_cast<unsigned>(BIM * BJM) + (BBX ? static_cast<unsigned>(TI * TJ) : 0u);
     static constexpr int SMEM_BYTES = S * STAGE_BYTES + 2 * S * 8;
     static constexpr int THREADS = 32 * (W + 1);
     static_assert(TI % 32 == 0 && BI <= 256 && BIM <= 256 && BJM <= 256, "TMA box limits");
@@ -110,7 +116,8 @@ __device__ __forceinline__ constexpr int own_index(int k, int li, int cj) {
 
 template <class M, int COLL, class CFG>
 __global__ void __launch_bounds__(CFG::THREADS, 1)
-    k_step_tma(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap mmap, Geometry g,
+    k_step_tma(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap mmap,
+               const __grid_constant__ CUtensorMap bmap, Geometry g,
                OpenTable ot, Collision c, const typename M::T* __restrict__ fin, typename M::T* __restrict__ fout,
                StepSync ss) {
     using T = typename M::T;
@@ -154,6 +161,7 @@ __global__ void __launch_bounds__(CFG::THREADS, 1)
                 tma_load_3d(st + k * CFG::PLANE_BYTES, &pmap, DI(k) == 1 ? i0 - CFG::A : i0, DJ(k) == 1 ? j0 - 1 : j0,
                             k, &full[s]);
             tma_load_2d(st + 9 * CFG::PLANE_BYTES, &mmap, i0 - 16, j0 - 1, &full[s]);
+            if constexpr (CFG::BBX) tma_load_2d(st + 9 * CFG::PLANE_BYTES + CFG::MASK_BYTES, &bmap, i0, j0, &full[s]);
         }
         // Do not leave with copies in flight: wait for the last fill of every stage.
         const long long issued = n;
@@ -196,10 +204,14 @@ __global__ void __launch_bounds__(CFG::THREADS, 1)
                     for (int k = 0; k < 9; ++k) f[k] = M::load(plane(k) + pulled_index<CFG>(k, li, cj));
                 } else {
                     f[0] = M::load(plane(0) + pulled_index<CFG>(0, li, cj));
+                    [[maybe_unused]] unsigned bbits = 0;
+                    if constexpr (CFG::BBX) bbits = (st + 9 * CFG::PLANE_BYTES + CFG::MASK_BYTES)[cj * TI + li];
 #pragma unroll
                     for (int k = 1; k < 9; ++k) {
                         // bounce-back source: this node's own value of direction opp(k)
-                        const bool bb = mask_class(sm[(cj + 1 - DJ(k)) * BIM + li + 16 - DI(k)]) == CLS_BB;
+                        bool bb;
+                        if constexpr (CFG::BBX) bb = (bbits >> (k - 1)) & 1u;
+                        else bb = mask_class(sm[(cj + 1 - DJ(k)) * BIM + li + 16 - DI(k)]) == CLS_BB;
                         const T* p = bb ? plane(opp(k)) + own_index<CFG>(opp(k), li, cj)
                                         : plane(k) + pulled_index<CFG>(k, li, cj);
                         f[k] = M::load(p);

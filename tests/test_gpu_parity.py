@@ -109,7 +109,7 @@ def test_f64_list_and_two_step_kernels_bit_exact(case, steps, pipeline):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
-@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("case", [CASES[2], CASES[5], CASES[6]], ids=[CASES[2][0], CASES[5][0], CASES[6][0]])
 def test_f64_every_step_kernel_bit_exact(case, pipeline):
     """The active-sector list (-2), the one-thread-per-node kernel (-1) and
@@ -131,7 +131,7 @@ def test_f64_pipeline_large_lattice_bit_exact():
     p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
     table = H.open_values(lists, "const:0.02:0", "pressure", 1)
     outs = []
-    for pipeline in (-1, -2, 0, 1, 2, 3, 4, 5):
+    for pipeline in (-1, -2, 0, 1, 2, 3, 4, 5, 6):
         outs.append(run_gpu(lists, p, 60, table, pipeline=pipeline))
     act = H.active_mask(lists)
     for o in outs[1:]:
@@ -157,7 +157,7 @@ def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
-@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3)], ids=["f32s", "f16s"])
 def test_shifted_storage_velocity_error(storage, tol, pipeline):
     lists = H.classify(H.channel_types(64, 160, discs=[(32, 40, 8)]))
@@ -178,7 +178,7 @@ def test_shifted_forms_equal_across_kernels(storage):
     lists = H.classify(H.porous_types(200, 300, fraction=0.25, rmin=2, rmax=6, seed=9))
     p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
     table = H.open_values(lists, "const:0.03:0", "pressure", 1)
-    outs = [run_gpu(lists, p, 101, table, storage=storage, pipeline=cfg) for cfg in (-1, -2, 0, 1, 2, 3, 4, 5)]
+    outs = [run_gpu(lists, p, 101, table, storage=storage, pipeline=cfg) for cfg in (-1, -2, 0, 1, 2, 3, 4, 5, 6)]
     act = H.active_mask(lists)
     for o in outs[1:]:
         np.testing.assert_array_equal(o["post"][:, act], outs[0]["post"][:, act])
@@ -197,8 +197,8 @@ def test_tune_pipeline_steps_are_ordinary_steps(storage):
         g.set_open_values(pressure_table(table, lists, p), 0)
         g.init()
         cfg, ms = g.tune_pipeline(8)
-        assert cfg in (-2, -1, 0, 1, 2, 3, 4, 5) and ms > 0.0 and g.pipeline == cfg
-        assert g.t == 1 + 2 * 8 * 8  # init + warm-up and timed steps of all 8 configurations
+        assert cfg in (-2, -1, 0, 1, 2, 3, 4, 5, 6) and ms > 0.0 and g.pipeline == cfg
+        assert g.t == 1 + 2 * 8 * 9  # init + warm-up and timed steps of all 9 configurations
         g.step(5, macro=True)
         steps = g.t
         got_pop, (got_rho, got_u) = g.post_collision(), g.macro()
