@@ -58,6 +58,17 @@ def test_format_matches_printf(tmp_path):
     assert read_pair(tmp_path, 7) == printf_text(u)
 
 
+def test_non_finite_values(tmp_path):
+    """A diverged run prints what ostream prints: nan, -nan, inf, -inf, -0."""
+    u = np.zeros((1, 5, 2))
+    u[0, :, 0] = [np.nan, -np.nan, np.inf, -np.inf, -0.0]
+    u[0, :, 1] = [1.0, 2.5, -3.25, 1e-7, 123456789.0]
+    assert np.signbit(u[0, 1, 0])
+    with L.OutputWriter(str(tmp_path)) as w:
+        w.save_host(u, 0)
+    assert read_pair(tmp_path, 0) == ["nan -nan inf -inf -0 \n", "1 2.5 -3.25 1e-07 1.23457e+08 \n"]
+
+
 def test_many_saves_one_slot_in_order(tmp_path):
     rng = np.random.default_rng(5)
     us = [rng.standard_normal((9, 5, 2)) for _ in range(12)]
