@@ -5,7 +5,7 @@
 // advances two steps per pass over HBM: for each tile of TI rows x TJ columns
 // the producer warp brings f*_{t-1} of the tile plus a two-node halo (all 9
 // planes, unshifted) and the node mask plus a three-node halo into a shared
-// memory stage with cp.async.bulk.tensor (no cluster multicast).  The consumer
+// memory stage with cp.async.bulk.tensor (each CTA loads its own boxes).  The consumer
 // warps then
 //   A. compute step t for the tile plus a one-node halo, (TI+2) x (TJ+2)
 //      nodes, into a shared-memory buffer `mid` (inactive nodes store their

@@ -4,7 +4,7 @@
 // the tiles; in each CTA one producer warp streams, for every tile, the 9
 // population boxes the tile pulls from (plane k shifted by -c_k) and the tile's
 // node-mask with a one-node halo into a ring of S shared-memory stages with
-// cp.async.bulk.tensor (no cluster multicast), completion tracked by mbarriers.
+// cp.async.bulk.tensor (each CTA loads its own boxes), completion tracked by mbarriers.
 // W consumer warps compute the tile's nodes from shared memory and store the
 // new post-collision populations straight to HBM.  The bytes in flight live in
 // shared memory instead of registers, so HBM stays busy with few warps.
