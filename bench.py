@@ -746,7 +746,8 @@ def main():
     ap.add_argument("--workload", default="porous4096",
                     choices=("porous4096", "cylinder1024x256", "cavity129", "cavity", "batch256", "serve"))
     ap.add_argument("--pipeline", type=int, default=None,
-                    help="plain path step kernel: -1 one thread per node, 0..2 TMA configurations (default: per lattice)")
+                    help="plain path step kernel: -1 one thread per node, -2 active-sector list, 0..2 and 6 TMA "
+                         "configurations, 3..5 two steps per pass (default: per lattice)")
     ap.add_argument("--launch-shape", type=int, default=None, help="columns per block of the one-thread kernel")
     ap.add_argument("--lattices", type=int, default=256,
                     help="batch256 workload: the first N of the 256 problems (smaller batches for profiling)")

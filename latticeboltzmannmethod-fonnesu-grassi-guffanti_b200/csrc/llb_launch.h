@@ -95,8 +95,8 @@ struct TmaPlan {
     int smem = 0;          // dynamic shared memory bytes
     int threads = 0;
 };
-// Configurations 0..2: one step per launch (k_step_tma); 3..5: two steps per
-// launch (k_step_pair); 6: one step per launch with the tile's bounce bytes.
+// Configurations 0..2 and 6: one step per launch (k_step_tma; 6 also loads the
+// tile's bounce bytes); 3..5: two steps per launch (k_step_pair).
 constexpr int TMA_CONFIGS = 7;
 constexpr int FIRST_PAIR_CONFIG = 3;
 // Fills `out` for configuration `cfg` (0..TMA_CONFIGS-1) of a storage form.

@@ -361,7 +361,9 @@ class CudaLattice:
         return float(ms.value)
 
     def set_pipeline(self, config: int):
-        """0..2: TMA-pipelined step configurations; -1: one thread per node."""
+        """-1: one thread per node; -2: the active-sector list; 0..2 and 6: TMA
+        pipeline configurations (6 also loads the tile's bounce bytes); 3..5:
+        two steps per pass through shared memory."""
         _check(lib().llb_set_pipeline(self._h, config), self._h)
 
     @property
