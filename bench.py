@@ -343,6 +343,108 @@ def drag_lift(L, wl, nodes, R, C, device, steps, every=100):
     return out
 
 
+def shifted_accuracy(L, wl, nodes, R, C, device, steps):
+    """Velocity error of the shifted storage forms against the FP64 run of the
+    same lattice after `steps` steps (config 3 states 20 000): relative L2
+    over the active nodes, u of both components, unrounded."""
+    act = np.zeros((C, R), dtype=bool)
+    for k in ("fluid", "inlet", "outlet"):
+        act[nodes[k][:, 1], nodes[k][:, 0]] = True
+    us = {}
+    for storage in (0, 1, 2):
+        g = make_lattice(L, wl, nodes, R, C, storage, device)
+        g.init()
+        g.step(steps - 1, macro=True)
+        g.check_numerics()
+        us[storage] = g.macro()[1][:, act]
+        g.close()
+    ref = us[0]
+    norm = float(np.sqrt((ref ** 2).sum()))
+    out = {"steps": steps, "lattice": wl["name"], "oracle": "the FP64 path on the GPU (bit-exact with the reference)"}
+    for storage, name in ((1, "f32s"), (2, "f16s")):
+        out[name] = {"u_rel_l2_vs_f64": float(np.sqrt(((us[storage] - ref) ** 2).sum())) / norm,
+                     "u_max_abs_diff": float(np.abs(us[storage] - ref).max())}
+    return out
+
+
+def open_flow(L, device, steps, warmup):
+    """The plain FP64 path on open flow: the 4096 x 4096 lid cavity (HBM-bound,
+    default kernel) and config 1 (129 x 129 cavity, L2-resident and
+    launch-bound: microseconds per step over 2000 graph-replayed steps)."""
+    class One:  # single-process timing (no ranks)
+        world = 1
+
+        @staticmethod
+        def barrier():
+            pass
+
+        @staticmethod
+        def max(x):
+            return x
+
+    out = {}
+    peak = (json.load(open(PEAKS_FILE)).get("hbm_gbs") if os.path.exists(PEAKS_FILE) else None) or FALLBACK_HBM_GBS
+    for name, size, k in (("cavity", 4096, max(steps, 100)), ("cavity129", 129, 2000)):
+        wl = workload(name, size)
+        types = wl["types"]()
+        nodes = L.classify(types)
+        R, C = types.shape
+        n_active = len(nodes["fluid"]) + len(nodes["inlet"]) + len(nodes["outlet"])
+        g, ms, _, _ = time_form(L, wl, nodes, R, C, 0, device, warmup, k, One)
+        per = ms / k
+        spp = 2 if g.pipeline in PAIR_CONFIGS else 1
+        bps = bytes_per_step(8, n_active, R * C, spp)
+        out[wl["name"]] = {"mlups": round(R * C / per / 1e3, 1), "us_per_step": round(per * 1e3, 3),
+                           "steps": k, "pipeline": g.pipeline, "gb_s": round(bps / per / 1e6, 1),
+                           "frac_of_measured_hbm": round(bps / per / 1e6 / peak, 4)}
+        g.close()
+    out["cavity129"]["note"] = "config 1: 16 641 nodes, L2-resident, launch-bound; the HBM fraction does not apply"
+    return out
+
+
+def reference_parity(L, wl, types, nodes, device, steps=3):
+    """The plain FP64 path against the reference itself on the bench's own
+    lattice: LLALBM's perform_lbm with the Serial policies
+    (oracle/_ref/ref_runner, the parity build without FMA contraction) for
+    `steps` steps, compared bit for bit with the CUDA path after the same
+    steps (populations S_t, u and rho of every node)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_runner")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_runner was not built"}
+    R, C = types.shape
+    with tempfile.TemporaryDirectory() as d:
+        raw = os.path.join(d, "types.u8")
+        np.ascontiguousarray(types.T).tofile(raw)
+        cmd = [exe, "--types-raw", raw, str(R), str(C), "--policy", "serial", *wl["ref_args"],
+               "--steps", str(steps), "--out", d]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, text=True, cwd=d, timeout=3600)
+        secs = time.perf_counter() - t0
+        if p.returncode != 0:
+            return {"unavailable": "reference runner failed: " + p.stderr[-200:]}
+        ref_pop = np.fromfile(os.path.join(d, "populations.f64")).reshape(9, C, R)
+        ref_u = np.fromfile(os.path.join(d, "u.f64")).reshape(2, C, R)
+        ref_rho = np.fromfile(os.path.join(d, "rho.f64")).reshape(C, R)
+    g = make_lattice(L, wl, nodes, R, C, 0, device)
+    g.init()
+    g.step(steps - 1, macro=True)
+    pop = g.populations()
+    rho, u = g.macro()
+    pipeline = g.pipeline
+    g.close()
+    act = np.zeros((C, R), dtype=bool)
+    for k in ("fluid", "inlet", "outlet"):
+        act[nodes[k][:, 1], nodes[k][:, 0]] = True
+    dpop = float(np.abs(pop[:, act] - ref_pop[:, act]).max())
+    return {"config": wl["name"], "steps": steps, "max_abs_df": dpop,
+            "max_abs_du": float(np.abs(u - ref_u).max()), "max_abs_drho": float(np.abs(rho - ref_rho).max()),
+            "bit_exact": bool(np.array_equal(pop[:, act], ref_pop[:, act]) and np.array_equal(u, ref_u)
+                              and np.array_equal(rho, ref_rho)),
+            "active_nodes": int(act.sum()), "gpu_pipeline": pipeline,
+            "reference": "LLALBM perform_lbm, SerialPolicy (BGK, BounceBack, ZouHe + Zou-He pressure policy), "
+                         "g++ -O2 -ffp-contract=off", "reference_seconds": round(secs, 1)}
+
+
 def run_ours(a, dist):
     import llalbm_cuda as L
 
@@ -354,7 +456,6 @@ def run_ours(a, dist):
     dev = dist.local
     sampler = ClockSampler(dev)
     forms = {}
-    u_ref = None
     head = None
     for storage, name, sb in ((0, "f64", 8), (1, "f32s", 4), (2, "f16s", 2)):
         if name not in a.forms.split(","):
@@ -367,14 +468,10 @@ def run_ours(a, dist):
         form = {"mlups": dist.world * R * C / per / 1e3, "ms_per_step": per, "gb_s": bps / per / 1e6,
                 "bytes_per_step": bps, "pipeline": g.pipeline, "steps_per_pass": spp}
         if storage == 0:
-            u_ref = u
             head = (g, ms, t0, t1)
         else:
-            act = np.zeros((C, R), dtype=bool)
-            for k in ("fluid", "inlet", "outlet"):
-                act[nodes[k][:, 1], nodes[k][:, 0]] = True
-            diff = u[:, act] - u_ref[:, act]
-            form["u_rel_l2_vs_f64"] = float(np.sqrt((diff ** 2).sum() / (u_ref[:, act] ** 2).sum()))
+            # the forms' velocity error is measured after the configuration's
+            # full step count (shifted_accuracy), not after these few steps
             g.close()
         forms[name] = form
     g, ms, t0, t1 = head
@@ -758,7 +855,9 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="porous workload: skip the batched and served summaries")
     ap.add_argument("--force-steps", type=int, default=50000,
-                    help="cylinder workload: steps of the drag/lift comparison of the storage forms (0: skip)")
+                    help="steps of the config-2 drag/lift comparison of the storage forms (0: skip)")
+    ap.add_argument("--accuracy-steps", type=int, default=20000,
+                    help="porous workload: steps of the shifted forms' velocity-error run against FP64")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -836,12 +935,25 @@ def main():
     if dist.world == 1 and a.workload == "porous4096" and not a.no_extras:
         import llalbm_cuda as L
         line["output_writer"] = output_writer(L, dist.local)
+        # the shifted forms' velocity error on config 3 as stated (20 000 steps)
+        nodes = L.classify(types)
+        R, C = types.shape
+        line["accuracy"] = shifted_accuracy(L, wl, nodes, R, C, dist.local, a.accuracy_steps)
+        # config 2's drag and lift of every storage form over its 50 000 steps
+        cwl = workload("cylinder1024x256")
+        ctypes_ = cwl["types"]()
+        line["drag_lift"] = drag_lift(L, cwl, L.classify(ctypes_), ctypes_.shape[0], ctypes_.shape[1], dist.local,
+                                      a.force_steps)
+        line["open_flow"] = open_flow(L, dist.local, a.steps, a.warmup)
     if dist.rank == 0:
         if dist.world == 1 and not a.no_cpu_baseline:
             cb = reference_cpu(wl, types, 1, 3 if a.workload == "porous4096" else 100)
             if cb is None or "error" in cb:
                 cb = oracle_cpu(wl, types, 2 if a.workload == "porous4096" else 100)
             line["cpu_baseline"] = cb
+            if a.workload == "porous4096" and not a.no_extras:
+                import llalbm_cuda as L
+                line["parity"] = reference_parity(L, wl, types, L.classify(types), dist.local)
         print(json.dumps(line), flush=True)
     dist.close()
 

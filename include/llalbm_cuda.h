@@ -176,7 +176,8 @@ int llb_get_post_collision(llb_handle h, double* populations);
 /* FlowAnalyzer<2>::compute_flow_properties (utils/analysis/FlowAnalyzer.hpp:348-451)
    over the resident post-collision state: per-point terms exactly as the
    reference, totals summed on the device with compensated FP64.
-   llb_set_force_points uploads the considered points once. */
+   llb_set_force_points uploads the considered points once (ij: 2 n
+   coordinates, dirs: n direction words). */
 int llb_set_force_points(llb_handle h, const int64_t* ij, const uint16_t* dirs, int64_t n);
 int llb_flow_forces(llb_handle h, double lift_drag[2]);
 /* Gathers, for each considered point and each set direction bit, the
@@ -190,13 +191,15 @@ int llb_gather_force_inputs(llb_handle h, double* values);
    up front under a fixed budget, or a host that must not trigger the
    device-wide synchronisation cudaMalloc/cudaFree can cause: the points and
    the per-block partial sums go to one static device array of
-   LLB_NOALLOC_MAX_FORCE_POINTS points (about 1.2 MB per device, reserved when
-   the library loads) instead of buffers allocated per call.  Same per-point
+   LLB_NOALLOC_MAX_FORCE_POINTS points (about 1.2 MB per device, held until
+   the process exits) instead of buffers allocated per call.  Same per-point
    terms and summation order as llb_flow_forces.  More than the maximum points
    fails with LLB_E_INVALID.  The first call on a device looks the array up
-   (cudaGetSymbolAddress) and should come before any stream capture on that
-   device.  All calls share the array: calls that overlap on the GPU race and
-   must be serialised by the caller. */
+   (cudaGetSymbolAddress); CUDA loads device code lazily, so that lookup is
+   where the array's memory is taken: make the first call before the loop that
+   must not allocate and before any stream capture on that device.  All calls
+   share the array: calls that overlap on the GPU race and must be serialised
+   by the caller.  ij holds 2 n coordinates and dirs n direction words. */
 #define LLB_NOALLOC_MAX_FORCE_POINTS 65536
 int llb_flow_forces_noalloc(llb_handle h, const int64_t* ij, const uint16_t* dirs, int64_t n,
                             double lift_drag[2]);
@@ -280,8 +283,16 @@ int llb_batch_get_config(llb_batch_handle b, int32_t* block_y, int32_t* steps_pe
 int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, int32_t* steps_per_launch,
                    float* ms_per_step);
 int llb_batch_get_step(llb_batch_handle b, int64_t* step);
-/* Waits for the batch; LLB_E_TIMEOUT if a cooperative launch gave up a grid barrier. */
+/* Waits for the batch; LLB_E_TIMEOUT if a cooperative launch gave up a grid
+   barrier.  The lattices' states are then unspecified (blocks that gave up
+   skipped their later steps): remove them and add them again.  The barrier
+   itself is reset, so the batch stays usable. */
 int llb_batch_synchronize(llb_batch_handle b);
+/* Polls of the cooperative launches' grid barrier before a block gives up and
+   the launch reports LLB_E_TIMEOUT (-1: the default, 2^22).  For tests of the
+   timeout path (0 makes every block but the last to arrive give up at once);
+   no reference counterpart. */
+int llb_batch_set_wait_limit(llb_batch_handle b, int64_t polls);
 /* Without waiting: *done = 1 when everything queued on the batch has run. */
 int llb_batch_query(llb_batch_handle b, int32_t* done);
 /* Scheduling priority of the batch's stream (CUDA stream priorities: a lower
@@ -381,6 +392,14 @@ int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* m
 /* Columns of lattice nodes per thread block of the one-thread-per-node kernel
    (1..8; each block is 32 rows x block_y columns). */
 int llb_set_launch_shape(llb_handle h, int32_t block_y);
+/* Polls of the pipelined kernels' (configurations 0..6) waits for their
+   shared-memory stages before they give up, flag LLB_E_TIMEOUT (read by
+   llb_check_numerics) and return (-1: the default, 2^24).  The wait for the
+   kernel's own copies in flight keeps the default, so a kernel never leaves
+   with copies outstanding.  For tests of the timeout path (0 gives up at
+   once); the state after a timed-out step is unspecified (re-run llb_init).
+   No reference counterpart. */
+int llb_set_wait_limit(llb_handle h, int64_t polls);
 /* Device bytes held by the handle. */
 int llb_device_bytes(llb_handle h, int64_t* bytes);
 /* Message for the last error on this handle (or the last global error for NULL). */

@@ -24,10 +24,6 @@ using namespace llb;
 
 namespace {
 constexpr int BATCH_GRAPH_STEPS = 32;  // even: a replay keeps every lattice's buffer parity
-// Lattices of at least this many nodes fill the GPU on their own: they are
-// stepped by their own launch of their default kernel (TMA pipeline or one
-// thread per node) inside the batch step instead of through the work list.
-constexpr int64_t SOLO_MIN_NODES = 1 << 20;
 }
 
 struct llb_batch {
@@ -38,7 +34,6 @@ struct llb_batch {
     std::vector<llb_handle> slot;        // nullptr: free slot
     std::vector<BatchLattice> desc;      // per slot
     std::vector<int> order;              // active slots in descriptor order
-    std::vector<int> solo;               // slots stepped by their own launches
     BatchLattice* d_desc = nullptr;
     int desc_cap = 0;
     int2* d_items = nullptr;
@@ -48,6 +43,7 @@ struct llb_batch {
     long long* d_sbase = nullptr;
     unsigned* d_bar = nullptr;           // [count, generation]
     unsigned* d_err = nullptr;
+    long long bar_limit = BARRIER_LIMIT;  // polls of the grid barrier before a block gives up
     int block_y = 4;
     int spl = 1;                         // steps per launch
     bool dirty = true;
@@ -105,7 +101,6 @@ int rebuild(llb_batch_handle b) {
     if (!b->dirty) return LLB_OK;
     drop_graph(b);
     b->order.clear();
-    b->solo.clear();
     std::vector<BatchLattice> dev;
     std::vector<int2> items;
     for (int s = 0; s < static_cast<int>(b->slot.size()); ++s) {
@@ -113,11 +108,9 @@ int rebuild(llb_batch_handle b) {
         const int idx = static_cast<int>(dev.size());
         b->order.push_back(s);
         dev.push_back(b->desc[s]);
+        // every lattice, large or small, is tiles of the one work list: one
+        // persistent launch advances the whole batch
         const BatchLattice& d = b->desc[s];
-        if (b->slot[s]->R * b->slot[s]->C >= SOLO_MIN_NODES) {
-            b->solo.push_back(s);
-            continue;
-        }
         const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
         for (int t = 0; t < d.nti * ntj; ++t) items.push_back(make_int2(idx, t));
     }
@@ -154,6 +147,7 @@ BatchLaunch launch_desc(llb_batch_handle b, long long soff, int steps) {
     L.steps = steps;
     L.bar = b->d_bar;
     L.err = b->d_err;
+    L.bar_limit = b->bar_limit;
     L.block_y = b->block_y;
     L.stream = b->stream;
     L.cooperative = steps > 1;
@@ -167,44 +161,28 @@ int set_base(llb_batch_handle b) {
     return LLB_OK;
 }
 
-// Own launches of the solo lattices for batch step b->step + soff (the step
-// base on the device holds b->step).
-int launch_solo(llb_batch_handle b, long long soff) {
-    for (int s : b->solo) {
-        const BatchLattice& d = b->desc[s];
-        const long long delta = b->step + soff - d.s0;
-        const int rc = handle_launch_step(b->slot[s], d.cur0 ^ static_cast<int>(delta & 1), b->d_sbase,
-                                          soff + d.t0 - d.s0);
-        if (rc != LLB_OK) return bfail(b, rc, std::string("solo lattice: ") + llb_last_error(b->slot[s]));
-    }
-    return LLB_OK;
-}
-
-// Every lattice one step: the work-list kernel and the solo launches.
+// Every lattice one step: one launch of the work-list kernel.
 int launch_one_step(llb_batch_handle b, long long soff) {
     if (b->n_items > 0) {
         cudaError_t e = launch_batch_step(b->storage, launch_desc(b, soff, 1));
         if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
     }
-    return launch_solo(b, soff);
+    return LLB_OK;
 }
 
 int launch_steps(llb_batch_handle b, int32_t nsteps) {
     int rc;
-    if (b->n_items == 0 && b->solo.empty()) {
+    if (b->n_items == 0) {
         b->step += nsteps;
         return LLB_OK;
     }
-    if (b->spl > 1 && b->n_items > 0) {
-        // cooperative launches of spl steps each for the work list, solo
-        // lattices step by step beside them
+    if (b->spl > 1) {
+        // cooperative launches of spl steps each
         while (nsteps > 0) {
             const int k = std::min<int>(nsteps, b->spl);
             if ((rc = set_base(b))) return rc;
             cudaError_t e = launch_batch_step(b->storage, launch_desc(b, 0, k));
             if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("batched kernel: ") + cudaGetErrorString(e));
-            for (int s = 0; s < k; ++s)
-                if ((rc = launch_solo(b, s))) return rc;
             b->step += k;
             nsteps -= k;
         }
@@ -314,6 +292,8 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
     if (!h->own_stream) return bfail(b, LLB_E_STATE, "lattice already belongs to a batch");
     if (h->d_ps) return bfail(b, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the single-lattice path");
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    // the batch's kernels step the dense planes
+    if (handle_leave_compact(h) != LLB_OK) return bfail(b, LLB_E_CUDA, llb_last_error(h));
     // the lattice works on the batch's stream from now on
     LLB_BCUDA(b, cudaStreamSynchronize(h->stream));
     cudaStreamDestroy(h->stream);
@@ -489,8 +469,24 @@ int llb_batch_synchronize(llb_batch_handle b) {
     unsigned err = 0;
     LLB_BCUDA(b, cudaMemcpy(&err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (err) {
-        cudaMemset(b->d_err, 0, sizeof(unsigned));
+        // blocks that gave up had counted themselves at the barrier: clear
+        // [count, generation] too, or the next launch's first barrier could
+        // let blocks through before all of them arrive
+        LLB_BCUDA(b, cudaMemset(b->d_bar, 0, 2 * sizeof(unsigned)));
+        LLB_BCUDA(b, cudaMemset(b->d_err, 0, sizeof(unsigned)));
         return bfail(b, LLB_E_TIMEOUT, "batched kernel gave up a grid barrier");
+    }
+    return LLB_OK;
+}
+
+int llb_batch_set_wait_limit(llb_batch_handle b, int64_t polls) {
+    if (!b || polls < -1) return LLB_E_INVALID;
+    const long long lim = polls < 0 ? BARRIER_LIMIT : static_cast<long long>(polls);
+    if (lim != b->bar_limit) {
+        if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+        LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+        drop_graph(b);  // the limit is a kernel argument captured in the graphs
+        b->bar_limit = lim;
     }
     return LLB_OK;
 }

@@ -35,8 +35,11 @@ struct BatchLattice {
 constexpr long long BARRIER_LIMIT = 1LL << 22;
 constexpr unsigned BATCH_FLAG_TIMEOUT = 1u;
 
-// Generation barrier across the grid (blocks must be co-resident).
-__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks) {
+// Generation barrier across the grid (blocks must be co-resident); a block
+// gives up after `limit` polls.  A block that gave up has counted itself, so
+// the host clears [count, generation] before the next launch (the batch's
+// error path).
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, long long limit) {
     __shared__ int ok_sh;
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -51,7 +54,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, uns
         } else {
             long long it = 0;
             while (*vgen == g0) {
-                if (++it > BARRIER_LIMIT) { ok = 0; break; }
+                if (++it > limit) { ok = 0; break; }
                 __nanosleep(64);
             }
         }
@@ -114,7 +117,7 @@ template <class M>
 __global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __restrict__ lats,
                                                        const int2* __restrict__ items, int n_items,
                                                        const long long* sbase, long long soff, int steps,
-                                                       unsigned* bar, unsigned* err) {
+                                                       unsigned* bar, unsigned* err, long long bar_limit) {
     const long long s0 = *sbase + soff;
     for (int st = 0; st < steps; ++st) {
         const long long s = s0 + st;
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __
             batch_tile<M>(lats + it.x, it.y, s);
             it = it_next;
         }
-        if (st + 1 < steps && !grid_barrier(bar, bar + 1, gridDim.x)) {
+        if (st + 1 < steps && !grid_barrier(bar, bar + 1, gridDim.x, bar_limit)) {
             if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(err, BATCH_FLAG_TIMEOUT);
             return;
         }

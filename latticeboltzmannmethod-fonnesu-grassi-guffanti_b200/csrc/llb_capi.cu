@@ -86,6 +86,7 @@ LaunchCtx make_ctx(llb_handle h) {
     x.ss.tbase = nullptr;
     x.ss.t_off = h->step;
     x.ss.flags = h->d_flags;
+    x.ss.wait_limit = h->wait_limit;
     x.stream = h->stream;
     x.block_y = h->block_y;
     return x;
@@ -98,7 +99,8 @@ void release(llb_handle h) {
     for (auto& g : h->graph)
         if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_ps, h->d_psb, h->d_sectors, h->d_smask, h->d_sbb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
-                    h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather};
+                    h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather,
+                    h->cf[0], h->cf[1], h->d_cnb, h->d_cseg, h->d_cchunk, h->d_ccol, h->d_cinfo};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (auto& e : h->ev)
@@ -288,6 +290,196 @@ int steps_per_launch(llb_handle h) {
     return h->tma_cfg >= 0 && tma_plan(h->storage, h->tma_cfg, &p) && p.pair ? 2 : 1;
 }
 
+// ---------------------------------------------------------------------------
+// column-compacted storage (pipeline PIPE_COMPACT)
+// ---------------------------------------------------------------------------
+CompactGeo compact_geo(llb_handle h) {
+    CompactGeo cg{};
+    cg.info = h->d_cinfo;
+    cg.nb = h->d_cnb;
+    cg.seg = h->d_cseg;
+    cg.chunk = h->d_cchunk;
+    cg.col = h->d_ccol;
+    cg.nseg = h->cnseg;
+    cg.n_chunks = h->c_chunks;
+    cg.n_slots = h->c_slots;
+    cg.cplane = h->cplane;
+    return cg;
+}
+
+// The state's copy in the dense planes, after steps on the compacted ones.
+int state_to_dense(llb_handle h) {
+    if (h->where != RES_COMPACT) return LLB_OK;
+    cudaError_t e = launch_compact_copy(h->storage, make_ctx(h), compact_geo(h), h->f[h->cur], h->cf[h->cur], false);
+    if (e != cudaSuccess) return cuda_fail(h, e, "compacted-to-dense copy");
+    h->where = RES_BOTH;
+    return LLB_OK;
+}
+
+// The state's copy in the compacted planes, before compacted steps.
+int state_to_compact(llb_handle h) {
+    if (h->where != RES_DENSE) return LLB_OK;
+    cudaError_t e = launch_compact_copy(h->storage, make_ctx(h), compact_geo(h), h->f[h->cur], h->cf[h->cur], true);
+    if (e != cudaSuccess) return cuda_fail(h, e, "dense-to-compacted copy");
+    h->where = RES_BOTH;
+    return LLB_OK;
+}
+
+void release_compact(llb_handle h) {
+    for (void* p : {h->cf[0], h->cf[1], static_cast<void*>(h->d_cnb), static_cast<void*>(h->d_cseg),
+                    static_cast<void*>(h->d_cchunk), static_cast<void*>(h->d_ccol), static_cast<void*>(h->d_cinfo)})
+        if (p) cudaFree(p);
+    h->cf[0] = h->cf[1] = nullptr;
+    h->d_cnb = nullptr;
+    h->d_cseg = nullptr;
+    h->d_cchunk = nullptr;
+    h->d_ccol = nullptr;
+    h->d_cinfo = nullptr;
+    h->bytes -= h->compact_bytes;
+    h->compact_bytes = 0;
+    h->c_chunks = 0;
+    h->cplane = 0;
+    h->c_slots = 0;
+}
+
+// Compacted planes and their tables from the node mask and bounce bytes
+// (dense (j * ld + i) layout).  Slots are taken column by column, rows in
+// order; each column's run is padded to a whole 32-byte sector.
+int build_compact_from(llb_handle h, const std::vector<uint8_t>& mask, const std::vector<uint8_t>& bb) {
+    if (h->d_cseg) return LLB_OK;
+    if (h->d_ps) return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
+    const int64_t R = h->R, C = h->C, ld = h->ld;
+    const int64_t nseg = (R + 31) / 32;
+    const int64_t pad = 32 / static_cast<int64_t>(h->elem);
+    std::vector<int2> seg(static_cast<size_t>(C * nseg));
+    std::vector<int32_t> col(static_cast<size_t>(C + 1));
+    std::vector<uint16_t> info;
+    info.reserve(static_cast<size_t>(h->n_active + C * pad));
+    std::vector<int2> chunks;
+    int64_t t = 0;
+    for (int64_t j = 0; j < C; ++j) {
+        if (t + R + pad >= (int64_t{1} << 31))
+            return fail(h, LLB_E_UNSUPPORTED, "compacted planes need fewer than 2^31 slots");
+        col[static_cast<size_t>(j)] = static_cast<int32_t>(t);
+        int64_t in_col = 0;
+        for (int64_t s = 0; s < nseg; ++s) {
+            uint32_t m = 0;
+            const int64_t t_seg = t;
+            for (int64_t r = 0; r < 32 && 32 * s + r < R; ++r) {
+                const int64_t i = 32 * s + r;
+                const uint8_t mk = mask[static_cast<size_t>(j * ld + i)];
+                if (!class_active(mask_class(mk))) continue;
+                m |= 1u << r;
+                uint8_t mb = mk;
+                if (mask_class(mk) == CLS_FLUID && !(mk & MASK_PLAIN)) {
+                    // fluid nodes never lie on the lattice edge: every source is in range
+                    for (int k = 1; k < 9; ++k) {
+                        const int64_t si = i - DI(k), sj = j - DJ(k);
+                        if (mask_class(mask[static_cast<size_t>(sj * ld + si)]) == CLS_DEAD) mb |= COMPACT_DEAD_SRC;
+                    }
+                }
+                info.push_back(static_cast<uint16_t>(mb | (bb[static_cast<size_t>(j * ld + i)] << 8)));
+                if (in_col % 32 == 0) chunks.push_back(make_int2(static_cast<int>(j), static_cast<int>(i)));
+                ++in_col;
+                ++t;
+            }
+            seg[static_cast<size_t>(j * nseg + s)] = make_int2(static_cast<int>(m), static_cast<int>(t_seg));
+        }
+        while (t % pad) {
+            info.push_back(0);
+            ++t;
+        }
+    }
+    col[static_cast<size_t>(C)] = static_cast<int32_t>(t);
+    if (chunks.empty()) return fail(h, LLB_E_UNSUPPORTED, "no active node");
+    if (static_cast<uint64_t>(ld) * static_cast<uint64_t>(C) > 0xffffffffull)
+        return fail(h, LLB_E_UNSUPPORTED, "compacted planes need fewer than 2^32 dense slots per plane");
+    // neighbour offsets of every slot (dense index for nodes whose pull tests each source)
+    auto slot_at = [&](int64_t j, int64_t i) -> int64_t {
+        const int2 e = seg[static_cast<size_t>(j * nseg + (i >> 5))];
+        const uint32_t below_i = (i & 31) ? (static_cast<uint32_t>(e.x) & ((1u << (i & 31)) - 1u)) : 0u;
+        return e.y + __builtin_popcount(below_i);
+    };
+    std::vector<uint32_t> nb(info.size(), 0);
+    for (int64_t j = 0; j < C; ++j) {
+        int64_t q = col[static_cast<size_t>(j)];
+        for (int64_t i = 0; i < R; ++i) {
+            const uint8_t mk = mask[static_cast<size_t>(j * ld + i)];
+            if (!class_active(mask_class(mk))) continue;
+            const uint8_t mb = static_cast<uint8_t>(info[static_cast<size_t>(q)] & 0xffu);
+            if (mask_class(mk) == CLS_OPEN || (mb & COMPACT_DEAD_SRC)) {
+                nb[static_cast<size_t>(q)] = static_cast<uint32_t>(j * ld + i);
+            } else {
+                const int64_t dl = q - slot_at(j - 1, i), dr = slot_at(j + 1, i) - q;
+                if (dl < 0 || dl > 0xffff || dr < 0 || dr > 0xffff)
+                    return fail(h, LLB_E_UNSUPPORTED, "compacted planes: neighbour columns more than 65535 slots apart");
+                nb[static_cast<size_t>(q)] = static_cast<uint32_t>(dl) | (static_cast<uint32_t>(dr) << 16);
+            }
+            ++q;
+        }
+    }
+    const int64_t align = 256 / static_cast<int64_t>(h->elem);
+    const long long cplane = static_cast<long long>((t + align - 1) / align * align);
+    const int64_t before = h->bytes;
+    void* cf0 = nullptr;
+    void* cf1 = nullptr;
+    int2 *d_seg = nullptr, *d_chunk = nullptr;
+    int32_t* d_col = nullptr;
+    uint16_t* d_info = nullptr;
+    uint32_t* d_nb = nullptr;
+    const size_t pbytes = static_cast<size_t>(cplane) * 9 * h->elem;
+    int rc = dev_alloc(h, &cf0, pbytes);
+    if (!rc) rc = dev_alloc(h, &cf1, pbytes);
+    if (!rc) rc = dev_alloc(h, &d_seg, seg.size() * sizeof(int2));
+    if (!rc) rc = dev_alloc(h, &d_chunk, chunks.size() * sizeof(int2));
+    if (!rc) rc = dev_alloc(h, &d_col, col.size() * sizeof(int32_t));
+    if (!rc) rc = dev_alloc(h, &d_info, info.size() * sizeof(uint16_t));
+    if (!rc) rc = dev_alloc(h, &d_nb, nb.size() * sizeof(uint32_t));
+    cudaError_t e = cudaSuccess;
+    if (!rc) e = cudaMemcpyAsync(d_seg, seg.data(), seg.size() * sizeof(int2), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess)
+        e = cudaMemcpyAsync(d_chunk, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess)
+        e = cudaMemcpyAsync(d_col, col.data(), col.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess)
+        e = cudaMemcpyAsync(d_info, info.data(), info.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess)
+        e = cudaMemcpyAsync(d_nb, nb.data(), nb.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
+    if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(h, e, "compacted-plane tables upload");
+    if (rc) {
+        for (void* p : {cf0, cf1, static_cast<void*>(d_seg), static_cast<void*>(d_chunk), static_cast<void*>(d_col),
+                        static_cast<void*>(d_info), static_cast<void*>(d_nb)})
+            if (p) cudaFree(p);
+        h->bytes = before;
+        return rc;
+    }
+    h->cf[0] = cf0;
+    h->cf[1] = cf1;
+    h->d_cseg = d_seg;
+    h->d_cchunk = d_chunk;
+    h->d_ccol = d_col;
+    h->d_cinfo = d_info;
+    h->d_cnb = d_nb;
+    h->c_slots = static_cast<long long>(t);
+    h->cnseg = static_cast<int>(nseg);
+    h->c_chunks = static_cast<int>(chunks.size());
+    h->cplane = cplane;
+    h->compact_bytes = h->bytes - before;
+    return LLB_OK;
+}
+
+// As above, with the mask and bounce bytes read back from the device.
+int build_compact(llb_handle h) {
+    if (h->d_cseg) return LLB_OK;
+    const size_t n = static_cast<size_t>(h->ld) * h->C;
+    std::vector<uint8_t> mask(n), bb(n);
+    LLB_CUDA(h, cudaMemcpyAsync(mask.data(), h->d_mask, n, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaMemcpyAsync(bb.data(), h->d_bb, n, cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    return build_compact_from(h, mask, bb);
+}
+
 // One step kernel (two steps for a two-step configuration unless `single`).
 // Inside a graph capture the step index is relative (graph_offset >= 0, base
 // read from d_step); otherwise it is absolute.
@@ -296,6 +488,13 @@ int launch_one(llb_handle h, bool macro, long long graph_offset = -1, bool singl
     if (graph_offset >= 0) {
         x.ss.tbase = h->d_step;
         x.ss.t_off = graph_offset;
+    }
+    if (!macro && h->tma_cfg == PIPE_COMPACT) {
+        cudaError_t e = launch_step_compact(h->storage, x, compact_geo(h), h->cf[h->cur], h->cf[h->cur ^ 1]);
+        if (e != cudaSuccess) return cuda_fail(h, e, "compacted step kernel launch");
+        h->cur ^= 1;
+        ++h->step;
+        return LLB_OK;
     }
     if (!macro && h->tma_cfg >= 0) {
         int rc = build_maps(h);
@@ -359,6 +558,13 @@ int batch_max_grid(int s, int block_y, int sm_count) {
 cudaError_t launch_macro_now(int s, const LaunchCtx& x, const void* fin, long long t, double* rho, double* u) {
     return s == LLB_STORE_F64 ? launch_macro_now_f64(x, fin, t, rho, u) : launch_macro_now_lowp(s, x, fin, t, rho, u);
 }
+cudaError_t launch_step_compact(int s, const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
+    return s == LLB_STORE_F64 ? launch_step_compact_f64(x, cg, fin, fout) : launch_step_compact_lowp(s, x, cg, fin, fout);
+}
+cudaError_t launch_compact_copy(int s, const LaunchCtx& x, const CompactGeo& cg, void* dense, void* comp, bool to_compact) {
+    return s == LLB_STORE_F64 ? launch_compact_copy_f64(x, cg, dense, comp, to_compact)
+                              : launch_compact_copy_lowp(s, x, cg, dense, comp, to_compact);
+}
 cudaError_t launch_fill_keep(int s, const LaunchCtx& x, void* buf) {
     return s == LLB_STORE_F64 ? launch_fill_keep_f64(x, buf) : launch_fill_keep_lowp(s, x, buf);
 }
@@ -399,6 +605,7 @@ int handle_force_context(llb_handle h, LaunchCtx* ctx, const void** fin, double*
     if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
     int rc = select_device(h);
     if (rc) return rc;
+    if ((rc = state_to_dense(h))) return rc;
     *ctx = make_ctx(h);
     *fin = h->f[h->cur];
     *d_out = h->d_red;
@@ -409,24 +616,22 @@ int handle_force_context(llb_handle h, LaunchCtx* ctx, const void** fin, double*
     return LLB_OK;
 }
 int handle_fail(llb_handle h, int code, const char* msg) { return fail(h, code, msg); }
-int handle_launch_step(llb_handle h, int cur, const long long* tbase, long long t_off) {
-    LaunchCtx x = make_ctx(h);
-    x.ss.tbase = tbase;
-    x.ss.t_off = t_off;
-    cudaError_t e;
-    if (h->tma_cfg >= 0 && steps_per_launch(h) == 1) {
-        int rc = build_maps(h);
-        if (rc) return rc;
-        const long long ntiles = ((h->R + h->plan.TI - 1) / h->plan.TI) * ((h->C + h->plan.TJ - 1) / h->plan.TJ);
-        const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(h->sm_count) * h->plan.ctas_per_sm));
-        e = launch_step_tma(h->storage, h->plan, x, &h->pmap[cur], &h->mmap, &h->bmap, h->f[cur], h->f[cur ^ 1],
-                            grid);
-    } else {  // one step at a time in a batch: a two-step configuration uses the one-thread kernel
-        e = launch_step(h->storage, x, h->f[cur], h->f[cur ^ 1], false, false);
-    }
-    return e == cudaSuccess ? LLB_OK : cuda_fail(h, e, "step kernel launch");
-}
 LaunchCtx handle_ctx(llb_handle h) { return make_ctx(h); }
+int handle_dense_state(llb_handle h) { return state_to_dense(h); }
+int handle_leave_compact(llb_handle h) {
+    int rc = select_device(h);
+    if (rc) return rc;
+    if ((rc = state_to_dense(h))) return rc;
+    h->where = RES_DENSE;
+    if (h->tma_cfg != PIPE_COMPACT) return LLB_OK;
+    LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (auto& g : h->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    h->tma_cfg = default_dense_pipeline(*h);
+    h->maps_ready = false;
+    release_compact(h);
+    return LLB_OK;
+}
 }  // namespace llb
 
 // ---------------------------------------------------------------------------
@@ -541,6 +746,11 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "lattice upload"));
+    if (h->tma_cfg == PIPE_COMPACT && build_compact_from(h, mask, bb) != LLB_OK) {
+        // the dense kernels serve every lattice: fall back to their default
+        h->tma_cfg = default_dense_pipeline(*h);
+        h->err.clear();
+    }
     *out = h;
     return LLB_OK;
 }
@@ -584,6 +794,7 @@ int llb_init(llb_handle h, uint32_t flags) {
     h->step = 1;
     h->initialized = true;
     h->macro_valid = macro;
+    h->where = RES_DENSE;
     return LLB_OK;
 }
 
@@ -595,6 +806,9 @@ int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
     if (rc) return rc;
     const bool macro = (flags & LLB_STEP_MACRO) != 0;
     int32_t plain = macro ? nsteps - 1 : nsteps;
+    const bool compact = h->tma_cfg == PIPE_COMPACT;
+    if (plain > 0 && (rc = compact ? state_to_compact(h) : state_to_dense(h))) return rc;
+    if (plain > 0) h->where = compact ? RES_COMPACT : RES_DENSE;  // where the steps below leave it
     if (plain >= GRAPH_STEPS) {
         cudaGraphExec_t g = nullptr;
         if ((rc = graph_for(h, &g))) return rc;
@@ -611,7 +825,10 @@ int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
         if ((rc = launch_one(h, false))) return rc;
     if (plain > 0 && (rc = launch_one(h, false, -1, true))) return rc;
     if (macro) {
+        // output steps write rho and u from the dense kernel
+        if ((rc = state_to_dense(h))) return rc;
         if ((rc = launch_one(h, true))) return rc;
+        h->where = RES_DENSE;
         h->macro_valid = true;
     }
     return LLB_OK;
@@ -640,6 +857,7 @@ int llb_compute_macro(llb_handle h, double* rho, double* u) {
     if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
     int rc = select_device(h);
     if (rc) return rc;
+    if ((rc = state_to_dense(h))) return rc;
     LaunchCtx x = make_ctx(h);
     cudaError_t e = launch_macro_now(h->storage, x, h->f[h->cur], h->step, h->d_rho, h->d_u);
     if (e != cudaSuccess) return cuda_fail(h, e, "macro kernel launch");
@@ -655,6 +873,7 @@ static int dense_out(llb_handle h, double* host, bool finalize) {
     if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
     int rc = select_device(h);
     if (rc) return rc;
+    if ((rc = state_to_dense(h))) return rc;
     const size_t bytes = sizeof(double) * 9 * static_cast<size_t>(h->R * h->C);
     if (!h->d_dense && (rc = dev_alloc(h, &h->d_dense, bytes))) return rc;
     LaunchCtx x = make_ctx(h);
@@ -698,7 +917,8 @@ int llb_flow_forces(llb_handle h, double lift_drag[2]) {
     if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
     int rc = select_device(h);
     if (rc) return rc;
-    const int nb = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(148 * 4, (h->n_fpts + 255) / 256)));
+    if ((rc = state_to_dense(h))) return rc;
+    const int nb = force_blocks(h->n_fpts);
     if ((rc = ensure_partials(h, nb))) return rc;
     LaunchCtx x = make_ctx(h);
     cudaError_t e = launch_flow_forces(h->storage, x, h->f[h->cur], h->d_fpts, h->d_fdirs, h->n_fpts, h->d_partials, nb, h->d_red);
@@ -714,6 +934,7 @@ int llb_gather_force_inputs(llb_handle h, double* values) {
     if (h->n_fpts == 0) return LLB_OK;
     int rc = select_device(h);
     if (rc) return rc;
+    if ((rc = state_to_dense(h))) return rc;
     LaunchCtx x = make_ctx(h);
     cudaError_t e = launch_gather_forces(h->storage, x, h->f[h->cur], h->d_fpts, h->d_fdirs, h->n_fpts, h->d_gather);
     if (e != cudaSuccess) return cuda_fail(h, e, "gather kernel launch");
@@ -727,6 +948,7 @@ int llb_mass_momentum(llb_handle h, double out[3]) {
     if (!h->initialized) return fail(h, LLB_E_STATE, "lattice not initialised");
     int rc = select_device(h);
     if (rc) return rc;
+    if ((rc = state_to_dense(h))) return rc;
     const int64_t N = h->R * h->C;
     const int nb = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(148 * 8, (N + 255) / 256)));
     if ((rc = ensure_partials(h, nb))) return rc;
@@ -840,14 +1062,18 @@ static int build_sector_list(llb_handle h) {
 }
 
 int llb_set_pipeline(llb_handle h, int32_t config) {
-    if (!h || config < PIPE_LIST || config >= TMA_CONFIGS)
-        return fail(h, LLB_E_INVALID, "config must be -2, -1 or in [0, 7)");
+    if (!h || config < PIPE_COMPACT || config >= TMA_CONFIGS)
+        return fail(h, LLB_E_INVALID, "config must be -3, -2, -1 or in [0, 7)");
     if (config != PIPE_GRID && h->d_ps)
         return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
+    if (config == PIPE_COMPACT && !h->own_stream)
+        return fail(h, LLB_E_STATE, "a lattice in a batch is stepped by the batch's kernels");
     if (config != h->tma_cfg) {
         int rc = select_device(h);
         if (rc) return rc;
         if (config == PIPE_LIST && (rc = build_sector_list(h))) return rc;
+        if (config == PIPE_COMPACT && (rc = build_compact(h))) return rc;
+        if (h->tma_cfg == PIPE_COMPACT && (rc = state_to_dense(h))) return rc;
         LLB_CUDA(h, cudaStreamSynchronize(h->stream));
         for (auto& g : h->graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
@@ -894,7 +1120,7 @@ int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* m
     const int original = h->tma_cfg;
     int chosen = original;
     float chosen_ms = -1.0f;
-    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, 0, 1, 2, 3, 4, 5, 6};
+    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, PIPE_COMPACT, 0, 1, 2, 3, 4, 5, 6};
     for (int cfg : kCandidates) {
         if (llb_set_pipeline(h, cfg) != LLB_OK) continue;  // not available for this lattice
         // warm-up (tensor maps, graphs), then the timed steps
@@ -923,8 +1149,23 @@ int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* m
     if (rc) return rc;
     if ((rc = llb_set_pipeline(h, chosen))) return rc;
     if (chosen != PIPE_LIST) release_sector_list(h);
+    if (chosen != PIPE_COMPACT) release_compact(h);
     if (best) *best = chosen;
     if (ms_per_step) *ms_per_step = chosen_ms < 0.0f ? 0.0f : chosen_ms / static_cast<float>(trial_steps);
+    return LLB_OK;
+}
+
+int llb_set_wait_limit(llb_handle h, int64_t polls) {
+    if (!h || polls < -1) return fail(h, LLB_E_INVALID, "polls must be >= 0, or -1 for the default");
+    const long long lim = polls < 0 ? DEFAULT_WAIT_LIMIT : static_cast<long long>(polls);
+    if (lim != h->wait_limit) {
+        int rc = select_device(h);
+        if (rc) return rc;
+        LLB_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (auto& g : h->graph)  // the limit is a kernel argument captured in the graphs
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        h->wait_limit = lim;
+    }
     return LLB_OK;
 }
 

@@ -9,6 +9,12 @@ cudaError_t launch_step_f64(const LaunchCtx& x, const void* fin, void* fout, boo
     return do_step<ModelF64>(x, fin, fout, init, macro);
 }
 cudaError_t launch_fill_keep_f64(const LaunchCtx& x, void* buf) { return do_fill_keep<ModelF64>(x, buf); }
+cudaError_t launch_step_compact_f64(const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
+    return do_step_compact<ModelF64>(x, cg, fin, fout);
+}
+cudaError_t launch_compact_copy_f64(const LaunchCtx& x, const CompactGeo& cg, void* dense, void* comp, bool to_compact) {
+    return do_compact_copy<ModelF64>(x, cg, dense, comp, to_compact);
+}
 cudaError_t launch_finalize_f64(const LaunchCtx& x, const void* fin, double* out, long long t) {
     return do_finalize<ModelF64>(x, fin, out, t);
 }

@@ -69,7 +69,27 @@ struct llb_lattice {
     int sm_count = 148;
     // active nodes with a wall, obstacle, dead or outside source (not PLAIN)
     int64_t n_active = 0, n_nonplain = 0;
+    // column-compacted planes of the active nodes (pipeline PIPE_COMPACT,
+    // built on first use) and their addressing tables
+    void* cf[2] = {nullptr, nullptr};
+    uint32_t* d_cnb = nullptr;
+    int2* d_cseg = nullptr;
+    int2* d_cchunk = nullptr;
+    int32_t* d_ccol = nullptr;
+    uint16_t* d_cinfo = nullptr;
+    int cnseg = 0, c_chunks = 0;
+    long long cplane = 0, c_slots = 0;
+    int64_t compact_bytes = 0;
+    // where the resident state f*[cur] lives: RES_DENSE, RES_COMPACT or both
+    int where = 0;
+    // polls of the pipelined kernels' stage waits before they give up
+    long long wait_limit = llb::DEFAULT_WAIT_LIMIT;
 };
+
+// Residence of the state (llb_lattice::where).  Steps of the compacted
+// pipeline leave it in the compacted planes; every other kernel reads and
+// writes the dense planes, and a copy brings the state across when needed.
+constexpr int RES_DENSE = 0, RES_COMPACT = 1, RES_BOTH = 2;
 
 // Default plain-step kernel of a lattice, from measurements on B200 (cavities,
 // channels, cylinders and porous media from 724^2 to 4096^2, every storage
@@ -86,10 +106,10 @@ struct llb_lattice {
 //    bytes);
 //  * otherwise one thread per node, which reads only active sectors and runs
 //    close to the copy bandwidth on open flow.
-constexpr int PIPE_GRID = -1, PIPE_LIST = -2;
+constexpr int PIPE_GRID = -1, PIPE_LIST = -2, PIPE_COMPACT = -3;
 constexpr int64_t TMA_MIN_NODES = 1 << 19;
 constexpr double TMA_MIN_NONPLAIN = 0.05;
-inline int default_pipeline(const llb_lattice& h) {
+inline int default_dense_pipeline(const llb_lattice& h) {
     const int64_t n = h.R * h.C;
     if (n < TMA_MIN_NODES || h.n_active == 0) return PIPE_GRID;
     if (static_cast<double>(h.n_nonplain) >= TMA_MIN_NONPLAIN * static_cast<double>(h.n_active))
@@ -98,15 +118,17 @@ inline int default_pipeline(const llb_lattice& h) {
     if (h.storage == LLB_STORE_F16S) return state >= static_cast<double>(int64_t{1} << 27) ? 0 : PIPE_GRID;
     return state >= static_cast<double>(int64_t{1} << 28) ? llb::FIRST_PAIR_CONFIG : PIPE_GRID;
 }
+inline int default_pipeline(const llb_lattice& h) { return default_dense_pipeline(h); }
 
 namespace llb {
 // Launch context of a handle's current state (defined in llb_capi.cu).
 LaunchCtx handle_ctx(llb_handle h);
 // Error reporting on a handle.
 int handle_fail(llb_handle h, int code, const char* msg);
-// One plain step of a handle owned by a batch, from buffer `cur` into
-// cur ^ 1, with the kernel the handle selects (TMA pipeline or one thread
-// per node); the step index is *tbase + t_off.  The handle's step counter
-// and buffer index are not touched (the batch derives them).
-int handle_launch_step(llb_handle h, int cur, const long long* tbase, long long t_off);
+// Brings the state of a handle into its dense planes (a copy when the last
+// steps ran on the compacted ones); LLB_OK or an error code.
+int handle_dense_state(llb_handle h);
+// Before a batch takes a handle: its state in the dense planes, and a handle
+// on the compacted pipeline moves to the one-thread-per-node kernel.
+int handle_leave_compact(llb_handle h);
 }  // namespace llb

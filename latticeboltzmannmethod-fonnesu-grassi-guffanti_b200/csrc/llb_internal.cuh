@@ -95,6 +95,41 @@ struct Geometry {
     int n_sectors;
 };
 
+// Column-compacted storage of the active nodes (pipeline PIPE_COMPACT).
+// Each population plane holds only the fluid and open nodes, column by
+// column, rows in order; a column's run starts on a 32-byte boundary (the
+// gap before the next column is padding).  Obstacle interiors and dead
+// regions take no slot, so a step reads and writes only the bytes of active
+// nodes.  Per slot t:
+//   info[t]  node mask byte | bounce byte << 8 (padding: 0, dead);
+//   nb[t]    fluid nodes: (t - cL) | (cR - t) << 16, where cL / cR is the slot
+//            of row i in the left / right column, or of the next active row
+//            below it when row i is not active there; then (i - 1, j -+ 1)
+//            sits at cL - 1 / cR - 1 and (i + 1, j -+ 1) right after row i's
+//            position; (i -+ 1, j) sit at t -+ 1.
+//            Open nodes and fluid nodes with a dead source: the dense index
+//            j * ld + i (their pull tests every source through seg).
+//   seg[j * nseg + s]  (.x) bit r set when row 32 s + r of column j is
+//            active, (.y) slot of the first active row at or after row 32 s;
+//            the slot of active row i is seg.y + popc(seg.x & (2^(i%32) - 1)).
+//   chunk[w] (.x) column, (.y) first active row of 32 consecutive slots of
+//            that column; col[j] first slot of column j (col[C] = slots used):
+//            the copies between the dense and the compacted planes.
+// A FLUID node whose sources include a dead node carries COMPACT_DEAD_SRC in
+// its mask byte (bit 3, the side field, unused by fluid nodes).
+constexpr uint8_t COMPACT_DEAD_SRC = 8;
+struct CompactGeo {
+    const uint16_t* __restrict__ info;
+    const uint32_t* __restrict__ nb;
+    const int2* __restrict__ seg;
+    const int2* __restrict__ chunk;
+    const int32_t* __restrict__ col;
+    int nseg;           // 32-row segments per column
+    int n_chunks;
+    long long n_slots;  // col[C]
+    long long cplane;   // slots per plane (multiple of 256 bytes)
+};
+
 struct OpenTable {
     const double2* __restrict__ vals;  // [cap][n_open]
     int n_open;
@@ -125,6 +160,11 @@ struct StepSync {
     const long long* tbase;
     long long t_off;
     unsigned* flags;    // bit 0: non-finite density seen
+    // polls of a pipelined kernel's mbarrier waits for its stages before it
+    // gives up (the drain of its own copies in flight always waits the full
+    // DEFAULT_WAIT_LIMIT)
+    long long wait_limit;
 };
+constexpr long long DEFAULT_WAIT_LIMIT = 1LL << 24;
 
 }  // namespace llb

@@ -6,6 +6,7 @@
 #include "llb_tma.cuh"
 #include "llb_pair.cuh"
 #include "llb_batch.cuh"
+#include "llb_compact.cuh"
 
 namespace llb {
 
@@ -47,6 +48,30 @@ cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, 
         else { if (macro) LLB_STEP(1, true, false); else LLB_STEP(1, false, false); }
     }
 #undef LLB_STEP
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_step_compact(const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
+    using T = typename M::T;
+    if (cg.n_slots <= 0) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((cg.n_slots + COMPACT_BLOCK - 1) / COMPACT_BLOCK);
+    const T* in = static_cast<const T*>(fin);
+    T* out = static_cast<T*>(fout);
+    if (x.c.model == 0) k_step_compact<M, 0><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, x.ot, x.c, in, out, x.ss);
+    else k_step_compact<M, 1><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, x.ot, x.c, in, out, x.ss);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t do_compact_copy(const LaunchCtx& x, const CompactGeo& cg, void* dense, void* comp, bool to_compact) {
+    using T = typename M::T;
+    if (cg.n_chunks <= 0) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((static_cast<long long>(cg.n_chunks) * 32 + COMPACT_BLOCK - 1) / COMPACT_BLOCK);
+    T* d = static_cast<T*>(dense);
+    T* c = static_cast<T*>(comp);
+    if (to_compact) k_compact_copy<M, true><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, d, c);
+    else k_compact_copy<M, false><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, d, c);
     return cudaGetLastError();
 }
 
@@ -149,7 +174,8 @@ cudaError_t do_batch_step(const BatchLaunch& b) {
     const dim3 block(BX, b.block_y);
     auto kern = k_batch_step<M>;
     if (!b.cooperative) {
-        kern<<<b.grid, block, 0, b.stream>>>(b.lats, b.items, b.n_items, b.sbase, b.soff, b.steps, b.bar, b.err);
+        kern<<<b.grid, block, 0, b.stream>>>(b.lats, b.items, b.n_items, b.sbase, b.soff, b.steps, b.bar, b.err,
+                                             b.bar_limit);
         return cudaGetLastError();
     }
     const BatchLattice* lats = b.lats;
@@ -160,7 +186,8 @@ cudaError_t do_batch_step(const BatchLaunch& b) {
     int steps = b.steps;
     unsigned* bar = b.bar;
     unsigned* err = b.err;
-    void* args[] = {&lats, &items, &n_items, &sbase, &soff, &steps, &bar, &err};
+    long long bar_limit = b.bar_limit;
+    void* args[] = {&lats, &items, &n_items, &sbase, &soff, &steps, &bar, &err, &bar_limit};
     return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kern), dim3(b.grid), block, args, 0, b.stream);
 }
 

@@ -33,6 +33,16 @@ cudaError_t launch_gather_forces(int storage, const LaunchCtx& ctx, const void* 
 
 cudaError_t launch_fill_keep(int storage, const LaunchCtx& ctx, void* buf);
 
+// Column-compacted storage (llb_compact.cuh): one plain step between compacted
+// planes, and copies between the dense and the compacted planes.
+cudaError_t launch_step_compact(int storage, const LaunchCtx& ctx, const CompactGeo& cg, const void* fin, void* fout);
+cudaError_t launch_compact_copy(int storage, const LaunchCtx& ctx, const CompactGeo& cg, void* dense, void* comp,
+                                bool to_compact);
+cudaError_t launch_step_compact_f64(const LaunchCtx&, const CompactGeo&, const void*, void*);
+cudaError_t launch_compact_copy_f64(const LaunchCtx&, const CompactGeo&, void*, void*, bool);
+cudaError_t launch_step_compact_lowp(int storage, const LaunchCtx&, const CompactGeo&, const void*, void*);
+cudaError_t launch_compact_copy_lowp(int storage, const LaunchCtx&, const CompactGeo&, void*, void*, bool);
+
 struct BatchLattice;
 // Batched step over a work list (llb_batch.cuh).  `cooperative` launches the
 // grid cooperatively (required when steps > 1).
@@ -45,6 +55,7 @@ struct BatchLaunch {
     int steps;
     unsigned* bar;
     unsigned* err;
+    long long bar_limit;   // polls of the grid barrier before a block gives up
     int grid;
     int block_y;
     bool cooperative;
@@ -109,6 +120,14 @@ cudaError_t launch_step_tma_f64(const TmaPlan&, const LaunchCtx&, const CUtensor
 bool tma_plan_lowp(int storage, int cfg, TmaPlan* out);
 cudaError_t launch_step_tma_lowp(int storage, const TmaPlan&, const LaunchCtx&, const CUtensorMap*,
                                  const CUtensorMap*, const CUtensorMap*, const void*, void*, int);
+
+// Blocks of the lift/drag reduction, at most: llb_flow_forces and
+// llb_flow_forces_noalloc size their grids by the same rule, so both fold the
+// per-block partial sums in the same order.
+constexpr int FORCE_MAX_BLOCKS = 148 * 4;
+inline int force_blocks(long long n) {
+    return static_cast<int>(n > 0 ? ((n + 255) / 256 < FORCE_MAX_BLOCKS ? (n + 255) / 256 : FORCE_MAX_BLOCKS) : 1);
+}
 
 inline dim3 node_grid(const Geometry& g, int bx, int by) {
     return dim3(static_cast<unsigned>((g.rows + bx - 1) / bx), static_cast<unsigned>((g.cols + by - 1) / by));

@@ -19,6 +19,14 @@ cudaError_t launch_step_lowp(int storage, const LaunchCtx& x, const void* fin, v
 cudaError_t launch_fill_keep_lowp(int storage, const LaunchCtx& x, void* buf) {
     LLB_DISPATCH((do_fill_keep<ModelF32S>(x, buf)), (do_fill_keep<ModelF16S>(x, buf)));
 }
+cudaError_t launch_step_compact_lowp(int storage, const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
+    LLB_DISPATCH((do_step_compact<ModelF32S>(x, cg, fin, fout)), (do_step_compact<ModelF16S>(x, cg, fin, fout)));
+}
+cudaError_t launch_compact_copy_lowp(int storage, const LaunchCtx& x, const CompactGeo& cg, void* dense, void* comp,
+                                     bool to_compact) {
+    LLB_DISPATCH((do_compact_copy<ModelF32S>(x, cg, dense, comp, to_compact)),
+                 (do_compact_copy<ModelF16S>(x, cg, dense, comp, to_compact)));
+}
 cudaError_t launch_finalize_lowp(int storage, const LaunchCtx& x, const void* fin, double* out, long long t) {
     LLB_DISPATCH((do_finalize<ModelF32S>(x, fin, out, t)), (do_finalize<ModelF16S>(x, fin, out, t)));
 }

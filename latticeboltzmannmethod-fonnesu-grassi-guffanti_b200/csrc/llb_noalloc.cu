@@ -8,7 +8,9 @@
 // stalling every other lattice in flight.  llb_set_force_points and
 // llb_flow_forces allocate device buffers for the considered points and the
 // per-block partial sums; this entry point instead keeps both in one
-// file-scope device array, reserved when the library is loaded.
+// file-scope device array.  CUDA loads the library's device code on a device
+// lazily, so the array is reserved there at the latest by the first call's
+// set-up below, not by any later call.
 //
 // The array is shared by every call in the process (per device) and holds
 // whatever the last call left there.  Nothing in it has to start at zero:
@@ -17,8 +19,12 @@
 // the same time) race on the array; callers must serialise them.
 //
 // Set-up: the first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it.  That first
-// call should come before any stream capture begins on the device.
+// cudaGetSymbolAddress (with that device current) and caches it; that lookup
+// is where the device memory is taken.  Make that first call before the loop
+// that must not allocate and before any stream capture begins on the device.
+// A cudaDeviceReset frees the array with every other allocation of the
+// context (the library's lattices included), so the cached address is only
+// valid while the context that looked it up lives.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,7 +37,7 @@
 namespace {
 
 constexpr long long MAX_POINTS = LLB_NOALLOC_MAX_FORCE_POINTS;
-constexpr int MAX_BLOCKS = 148 * 4;  // partial-sum slots (grid of the force kernel)
+constexpr int MAX_BLOCKS = llb::FORCE_MAX_BLOCKS;  // partial-sum slots (grid of the force kernel)
 constexpr size_t PTS_BYTES = sizeof(int64_t) * 2 * MAX_POINTS;
 constexpr size_t DIRS_BYTES = (sizeof(uint16_t) * MAX_POINTS + 255) / 256 * 256;
 constexpr size_t PARTIAL_BYTES = sizeof(double2) * 3 * MAX_BLOCKS;
@@ -97,7 +103,7 @@ extern "C" int llb_flow_forces_noalloc(llb_handle h, const int64_t* ij, const ui
         if (e != cudaSuccess) return handle_fail(h, LLB_E_CUDA, "copy of the force points failed");
     }
     // same grid rule as llb_flow_forces, so both sum in the same order
-    const int nb = static_cast<int>(n > 0 ? (n + 255) / 256 < MAX_BLOCKS ? (n + 255) / 256 : MAX_BLOCKS : 1);
+    const int nb = force_blocks(n);
     e = launch_flow_forces(storage, x, fin, d_pts, d_dirs, n, d_partials, nb, d_out);
     if (e == cudaSuccess) e = cudaMemcpyAsync(lift_drag, d_out, sizeof(double) * 2, cudaMemcpyDeviceToHost, x.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(x.stream);

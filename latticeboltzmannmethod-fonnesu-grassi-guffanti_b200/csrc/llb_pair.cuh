@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(CFG::THREADS, CFG::CPS)
         for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++n) {
             const int s = static_cast<int>(n % S);
             const unsigned round = static_cast<unsigned>(n / S);
-            if (n >= S && !mbar_wait(&empty[s], (round - 1) & 1u)) {
+            if (n >= S && !mbar_wait(&empty[s], (round - 1) & 1u, ss.wait_limit)) {
                 atomicOr(ss.flags, FLAG_TIMEOUT);
                 break;
             }
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(CFG::THREADS, CFG::CPS)
     bool bad = false;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++n) {
         const int s = static_cast<int>(n % S);
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], static_cast<unsigned>(n / S) & 1u));
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], static_cast<unsigned>(n / S) & 1u, ss.wait_limit));
         if (!ok && lane == 0) *abort_flag = 1;
         consumer_barrier(32 * W);
         if (*abort_flag) {

@@ -29,7 +29,7 @@
 
 namespace llb {
 
-constexpr long long WAIT_LIMIT = 1LL << 24;  // try_wait polls before giving up
+constexpr long long WAIT_LIMIT = DEFAULT_WAIT_LIMIT;  // try_wait polls before the drain gives up
 constexpr unsigned FLAG_TIMEOUT = 2u;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -55,9 +55,10 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Waits for the phase with the given parity to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-    for (long long it = 0; it < WAIT_LIMIT; ++it)
+// Waits for the phase with the given parity to complete, at most `limit`
+// polls; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit = WAIT_LIMIT) {
+    for (long long it = 0; it < limit; ++it)
         if (mbar_test(bar, parity)) return true;
     return false;
 }
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(CFG::THREADS, 1)
         for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++n) {
             const int s = static_cast<int>(n % S);
             const unsigned round = static_cast<unsigned>(n / S);
-            if (n >= S && !mbar_wait(&empty[s], (round - 1) & 1u)) {
+            if (n >= S && !mbar_wait(&empty[s], (round - 1) & 1u, ss.wait_limit)) {
                 atomicOr(ss.flags, FLAG_TIMEOUT);
                 ok = false;
                 break;
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(CFG::THREADS, 1)
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++n) {
         const int s = static_cast<int>(n % S);
         // warp-uniform outcome: the warp's later ballots need every lane
-        if (!__all_sync(0xffffffffu, mbar_wait(&full[s], static_cast<unsigned>(n / S) & 1u))) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[s], static_cast<unsigned>(n / S) & 1u, ss.wait_limit))) {
             if (lane == 0) atomicOr(ss.flags, FLAG_TIMEOUT);
             break;
         }

@@ -101,6 +101,7 @@ SIGNATURES = {
     "llb_get_pipeline": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_tune_pipeline": [_H, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
     "llb_set_launch_shape": [_H, ctypes.c_int32],
+    "llb_set_wait_limit": [_H, ctypes.c_int64],
     "llb_compute_macro": [_H, _P, _P],
     "llb_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_H)],
     "llb_batch_destroy": [_H],
@@ -118,6 +119,7 @@ SIGNATURES = {
     "llb_batch_synchronize": [_H],
     "llb_batch_query": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_batch_set_stream_priority": [_H, ctypes.c_int32],
+    "llb_batch_set_wait_limit": [_H, ctypes.c_int64],
     "llb_batch_event_record": [_H, ctypes.c_int32],
     "llb_batch_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
     "llb_batch_info": [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
@@ -326,6 +328,8 @@ class CudaLattice:
 
     def set_force_points(self, pts, dirs):
         p = _ij(pts); q = np.ascontiguousarray(np.asarray(dirs, dtype=np.uint16).reshape(-1))
+        if len(q) != len(p):
+            raise ValueError(f"{len(p)} force points but {len(q)} direction words")
         _check(lib().llb_set_force_points(self._h, _ptr(p), _ptr(q), len(p)), self._h)
         self._force_n = len(p)
 
@@ -337,6 +341,8 @@ class CudaLattice:
     def flow_forces_noalloc(self, pts, dirs):
         """Lift and drag without device allocation (static scratch, <= 65536 points)."""
         p = _ij(pts); q = np.ascontiguousarray(np.asarray(dirs, dtype=np.uint16).reshape(-1))
+        if len(q) != len(p):
+            raise ValueError(f"{len(p)} force points but {len(q)} direction words")
         out = np.zeros(2)
         _check(lib().llb_flow_forces_noalloc(self._h, _ptr(p), _ptr(q), len(p), _ptr(out)), self._h)
         return float(out[0]), float(out[1])
@@ -381,6 +387,11 @@ class CudaLattice:
 
     def set_launch_shape(self, block_y: int):
         _check(lib().llb_set_launch_shape(self._h, block_y), self._h)
+
+    def set_wait_limit(self, polls: int):
+        """Polls of the pipelined kernels' stage waits before they give up
+        (-1: default); for tests of the timeout path."""
+        _check(lib().llb_set_wait_limit(self._h, polls), self._h)
 
     def device_bytes(self) -> int:
         b = ctypes.c_int64()
@@ -486,6 +497,11 @@ class CudaBatch:
 
     def synchronize(self):
         _bcheck(lib().llb_batch_synchronize(self._b), self._b)
+
+    def set_wait_limit(self, polls: int):
+        """Polls of the cooperative launches' grid barrier before a block
+        gives up (-1: default); for tests of the timeout path."""
+        _bcheck(lib().llb_batch_set_wait_limit(self._b, polls), self._b)
 
     def record(self, slot: int):
         _bcheck(lib().llb_batch_event_record(self._b, slot), self._b)

@@ -6,7 +6,7 @@ from the reference tree.  The reference ships no numeric golden vectors for this
 path (its tests are smoke runs), so these files are the pinned answers the C
 oracle and the CUDA path are checked against where the reference tree is absent.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <LLALBM checkout>
 
 Geometries are written in the reference's lattice-file format from the same
 generators the tests use (tests/harness.py); config 1 uses the reference's own
@@ -83,7 +83,7 @@ def cases():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the LLALBM checkout (test/assets/lid-lattice.txt)")
     a = ap.parse_args()
     if not H.have_ref():
         sys.exit("oracle/_ref/ref_runner is missing: run `make -C oracle` with the reference tree present")

@@ -125,3 +125,68 @@ def test_cuda_policy_matches_serial_policy_ps_obstacle(tmp_path):
     np.testing.assert_array_equal(outs["cuda"]["populations"][act], outs["serial"]["populations"][act])
     np.testing.assert_array_equal(outs["cuda"]["u"], outs["serial"]["u"])
     np.testing.assert_array_equal(outs["cuda"]["rho"], outs["serial"]["rho"])
+
+
+REF_LID_BINS = [os.path.join(BIN, f"ref_lid_exec_{p}") for p in ("serial", "cuda")]
+needs_ref_lid = pytest.mark.skipif(not all(os.path.exists(b) for b in REF_LID_BINS),
+                                   reason="the reference's LidExecTest was not built (reference headers absent)")
+
+
+@needs_ref_lid
+@pytest.mark.gpu
+def test_reference_lid_exec_program_with_one_token_swapped(tmp_path):
+    """The reference's own program test/unit/LidExecTest.cpp (Lattice from
+    ../test/assets/lid-lattice.txt, BGK tau 0.6, lid u 0.2, perform_lbm(100)
+    saving u on every step), built as shipped and with only its
+    `using Parallel = SerialPolicy<2, Config>;` line switched to CUDAPolicy:
+    all 200 saved files are byte-identical.  The lattice file is written from
+    the config-1 generator, which equals the reference's asset token for
+    token."""
+    results = {}
+    for exe in REF_LID_BINS:
+        root = tmp_path / os.path.basename(exe)
+        (root / "test" / "assets").mkdir(parents=True)
+        H.write_lattice_file(str(root / "test" / "assets" / "lid-lattice.txt"), H.cavity_types(129))
+        (root / "build").mkdir()
+        p = subprocess.run([exe], cwd=root / "build", capture_output=True, text=True, timeout=900)
+        assert p.returncode == 0, p.stdout[-1000:] + p.stderr[-1000:]
+        results[exe] = root / "build" / "results"
+    ser, cud = (results[b] for b in REF_LID_BINS)
+    files = sorted(os.listdir(ser))
+    assert len(files) == 200 and sorted(os.listdir(cud)) == files
+    for f in files:
+        assert filecmp.cmp(ser / f, cud / f, shallow=False), f
+
+
+OMP_BINS = [os.path.join(BIN, f"lid_trt_omp_{p}") for p in ("omp", "cuda")]
+
+
+@pytest.mark.skipif(not all(os.path.exists(b) for b in OMP_BINS), reason="OpenMP-family example not built")
+@pytest.mark.gpu
+def test_cuda_policy_matches_omp_policy_trt(tmp_path):
+    """A program on the reference's OpenMP policy family (OMPTRT collision,
+    OMPBounceBack, OMPZouHe lid with a ramp, OMPDefaultEquilibrium) built with
+    OMPPolicy and run on 4 threads, and built with CUDAPolicy: populations,
+    u, rho and the saved u files are identical."""
+    lat = str(tmp_path / "lid.txt")
+    H.write_lattice_file(lat, H.cavity_types(129))
+    lists = H.classify(H.cavity_types(129))
+    outs = {}
+    for exe in OMP_BINS:
+        d = tmp_path / os.path.basename(exe)
+        d.mkdir()
+        env = dict(os.environ, OMP_NUM_THREADS="4")
+        p = subprocess.run([exe, lat, "800", "200", str(d)], cwd=d, capture_output=True, text=True, timeout=900,
+                           env=env)
+        assert p.returncode == 0, p.stdout[-1000:] + p.stderr[-1000:]
+        outs[exe] = {n: np.fromfile(d / (n + ".f64")) for n in ("populations", "u", "rho")}
+        outs[exe]["dir"] = d / "results"
+    omp, cud = (outs[b] for b in OMP_BINS)
+    act = active_flat(lists)
+    np.testing.assert_array_equal(cud["populations"][act], omp["populations"][act])
+    np.testing.assert_array_equal(cud["u"], omp["u"])
+    np.testing.assert_array_equal(cud["rho"], omp["rho"])
+    files = sorted(os.listdir(omp["dir"]))
+    assert len(files) == 8
+    for f in files:
+        assert filecmp.cmp(omp["dir"] / f, cud["dir"] / f, shallow=False), f

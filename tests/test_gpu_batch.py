@@ -205,3 +205,29 @@ def test_batch_f16s_matches_single_lattice():
             u = b.lattice(slot).compute_macro()[1]
             err = np.sqrt(((u - u1) ** 2).sum() / max((u1 ** 2).sum(), 1e-30))
             assert err <= 1e-6, (prob[0], err)
+
+
+def test_batch_barrier_timeout_reports_and_recovers():
+    """A cooperative multi-step launch whose grid barrier gives up at once
+    (wait limit 0: every block but the last to arrive) reports LLB_E_TIMEOUT
+    on synchronisation and leaves the barrier cleared: fresh lattices added
+    to the same batch then run bit-exact with the default limit."""
+    import llalbm_cuda as L
+
+    steps = 120
+    with L.CudaBatch(storage=L.STORE_F64) as b:
+        slots = [add(b, prob, steps + 2) for prob in PROBLEMS]
+        b.set_config(4, 8)
+        b.set_wait_limit(0)
+        b.step(16)
+        with pytest.raises(L.LLBError) as e:
+            b.synchronize()
+        assert e.value.code == -9
+        for s in slots:
+            b.remove(s)
+        b.set_wait_limit(-1)
+        slots = [add(b, prob, steps + 2) for prob in PROBLEMS]
+        b.step(steps - 1)
+        b.synchronize()
+        for slot, prob in zip(slots, PROBLEMS):
+            check_against_oracle(b.lattice(slot), prob, steps)

@@ -91,13 +91,13 @@ def test_f64_bit_exact(case, steps):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
-@pytest.mark.parametrize("pipeline", [-2, 3, 4, 5])
+@pytest.mark.parametrize("pipeline", [-3, -2, 3, 4, 5])
 @pytest.mark.parametrize("steps", [2, 7, 300])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
 def test_f64_list_and_two_step_kernels_bit_exact(case, steps, pipeline):
-    """The active-sector list kernel (-2) and the two-steps-per-launch
-    configurations (3-5; odd step counts end with a lone step, 300 steps run
-    through graph replays) on every case."""
+    """The compacted-plane kernel (-3), the active-sector list kernel (-2) and
+    the two-steps-per-launch configurations (3-5; odd step counts end with a
+    lone step, 300 steps run through graph replays) on every case."""
     name, lists, p, ins, outs = case
     table = H.open_values(lists, ins, outs, steps)
     ref = H.run_oracle(lists, p, steps, table)
@@ -109,11 +109,11 @@ def test_f64_list_and_two_step_kernels_bit_exact(case, steps, pipeline):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
-@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("pipeline", [-3, -2, -1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("case", [CASES[2], CASES[5], CASES[6]], ids=[CASES[2][0], CASES[5][0], CASES[6][0]])
 def test_f64_every_step_kernel_bit_exact(case, pipeline):
-    """The active-sector list (-2), the one-thread-per-node kernel (-1) and
-    every TMA pipeline configuration."""
+    """The compacted planes (-3), the active-sector list (-2), the
+    one-thread-per-node kernel (-1) and every TMA pipeline configuration."""
     name, lists, p, ins, outs = case
     steps = 150
     table = H.open_values(lists, ins, outs, steps)
@@ -131,7 +131,7 @@ def test_f64_pipeline_large_lattice_bit_exact():
     p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
     table = H.open_values(lists, "const:0.02:0", "pressure", 1)
     outs = []
-    for pipeline in (-1, -2, 0, 1, 2, 3, 4, 5, 6):
+    for pipeline in (-1, -3, -2, 0, 1, 2, 3, 4, 5, 6):
         outs.append(run_gpu(lists, p, 60, table, pipeline=pipeline))
     act = H.active_mask(lists)
     for o in outs[1:]:
@@ -157,7 +157,7 @@ def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
-@pytest.mark.parametrize("pipeline", [-2, -1, 0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("pipeline", [-3, -2, -1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3)], ids=["f32s", "f16s"])
 def test_shifted_storage_velocity_error(storage, tol, pipeline):
     lists = H.classify(H.channel_types(64, 160, discs=[(32, 40, 8)]))
@@ -178,7 +178,7 @@ def test_shifted_forms_equal_across_kernels(storage):
     lists = H.classify(H.porous_types(200, 300, fraction=0.25, rmin=2, rmax=6, seed=9))
     p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
     table = H.open_values(lists, "const:0.03:0", "pressure", 1)
-    outs = [run_gpu(lists, p, 101, table, storage=storage, pipeline=cfg) for cfg in (-1, -2, 0, 1, 2, 3, 4, 5, 6)]
+    outs = [run_gpu(lists, p, 101, table, storage=storage, pipeline=cfg) for cfg in (-1, -3, -2, 0, 1, 2, 3, 4, 5, 6)]
     act = H.active_mask(lists)
     for o in outs[1:]:
         np.testing.assert_array_equal(o["post"][:, act], outs[0]["post"][:, act])
@@ -197,14 +197,47 @@ def test_tune_pipeline_steps_are_ordinary_steps(storage):
         g.set_open_values(pressure_table(table, lists, p), 0)
         g.init()
         cfg, ms = g.tune_pipeline(8)
-        assert cfg in (-2, -1, 0, 1, 2, 3, 4, 5, 6) and ms > 0.0 and g.pipeline == cfg
-        assert g.t == 1 + 2 * 8 * 9  # init + warm-up and timed steps of all 9 configurations
+        assert cfg in (-3, -2, -1, 0, 1, 2, 3, 4, 5, 6) and ms > 0.0 and g.pipeline == cfg
+        assert g.t == 1 + 2 * 8 * 10  # init + warm-up and timed steps of all 10 configurations
         g.step(5, macro=True)
         steps = g.t
         got_pop, (got_rho, got_u) = g.post_collision(), g.macro()
     ref = H.run_oracle(lists, p, steps, table) if storage == 0 else run_gpu(lists, p, steps, table, storage=storage)
     act = H.active_mask(lists)
     np.testing.assert_array_equal(got_pop[:, act], ref["post"][:, act])
+    np.testing.assert_array_equal(got_u, ref["u"])
+    np.testing.assert_array_equal(got_rho, ref["rho"])
+
+
+@pytest.mark.parametrize("storage", [0, 1, 2], ids=["f64", "f32s", "f16s"])
+def test_compact_state_moves_between_layouts(storage):
+    """Steps on the compacted planes (-3) interleaved with everything that reads
+    the dense planes (populations, forces, mass, output steps) and with
+    switches to other kernels and back: the state is copied across whenever
+    needed, so the run equals one without switches (FP64: the oracle)."""
+    lists = H.classify(H.porous_types(150, 210, seed=5))
+    p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.03:0", "pressure", 1)
+    plan = [(-3, 7, False), (-3, 40, True), (-1, 3, False), (-3, 33, False), (1, 5, False), (-3, 1, True),
+            (-3, 64, False), (-2, 2, False)]
+    with make_gpu(lists, p, storage=storage) as g:
+        g.set_open_values(pressure_table(table, lists, p), 0)
+        g.init()
+        g.set_force_points(lists.obstacle, lists.obstacle_dirs)
+        for cfg, n, macro in plan:
+            g.set_pipeline(cfg)
+            g.step(n, macro=macro)
+            g.flow_forces()
+            g.mass_momentum()
+        g.set_pipeline(-3)
+        g.step(9, macro=True)
+        steps = g.t
+        got_pop, got_post, (got_rho, got_u) = g.populations(), g.post_collision(), g.macro()
+    ref = H.run_oracle(lists, p, steps, table) if storage == 0 else run_gpu(lists, p, steps, table, storage=storage,
+                                                                            pipeline=-1)
+    act = H.active_mask(lists)
+    np.testing.assert_array_equal(got_pop[:, act], ref["populations"][:, act])
+    np.testing.assert_array_equal(got_post[:, act], ref["post"][:, act])
     np.testing.assert_array_equal(got_u, ref["u"])
     np.testing.assert_array_equal(got_rho, ref["rho"])
 
@@ -323,3 +356,35 @@ def test_cylinder_drag_lift_shifted_f32_within_a_thousandth():
     lift32, drag32 = hist[L.STORE_F32S][:, 0], hist[L.STORE_F32S][:, 1]
     assert np.max(np.abs(drag32 - drag64) / np.abs(drag64)) <= 1e-3
     assert np.max(np.abs(lift32 - lift64)) <= 1e-3 * max(np.abs(lift64).max(), 1e-12)
+
+
+@pytest.mark.parametrize("pipeline", [1, 6, 3])
+def test_pipelined_wait_timeout_reports_and_recovers(pipeline):
+    """The TMA (1, 6) and two-steps-per-pass (3) kernels with their stage
+    waits limited to 0 polls give up at once: the flag comes back as
+    LLB_E_TIMEOUT, the kernel returns after its copies in flight have landed
+    (that wait keeps its full limit), and the same handle, re-initialised with
+    the default limit, runs bit-exact."""
+    import llalbm_cuda as L
+
+    lists = H.classify(H.porous_types(300, 400, seed=4))
+    p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.02:0", "pressure", 1)
+    steps = 64
+    ref = H.run_oracle(lists, p, steps, table)
+    with make_gpu(lists, p, pipeline=pipeline) as g:
+        g.set_open_values(pressure_table(table, lists, p), 0)
+        g.init()
+        g.set_wait_limit(0)
+        g.step(4)
+        with pytest.raises(L.LLBError) as e:
+            g.check_numerics()
+        assert e.value.code == -9
+        g.set_wait_limit(-1)
+        g.init()
+        g.step(steps - 1, macro=True)
+        g.check_numerics()
+        pop, (rho, u) = g.populations(), g.macro()
+    act = H.active_mask(lists)
+    np.testing.assert_array_equal(pop[:, act], ref["populations"][:, act])
+    np.testing.assert_array_equal(u, ref["u"])
