@@ -393,10 +393,13 @@ def open_flow(L, device, steps, warmup):
         g, ms, _, _ = time_form(L, wl, nodes, R, C, 0, device, warmup, k, One)
         per = ms / k
         spp = 2 if g.pipeline in PAIR_CONFIGS else 1
-        bps = bytes_per_step(8, n_active, R * C, spp)
+        bps = bytes_per_step(8, n_active, R * C)          # the metric's bytes of one step
         out[wl["name"]] = {"mlups": round(R * C / per / 1e3, 1), "us_per_step": round(per * 1e3, 3),
                            "steps": k, "pipeline": g.pipeline, "gb_s": round(bps / per / 1e6, 1),
                            "frac_of_measured_hbm": round(bps / per / 1e6 / peak, 4)}
+        if spp == 2:
+            out[wl["name"]]["note"] = ("two steps per pass: the kernel moves the bytes of one step per two steps, "
+                                       "so its own DRAM traffic is half of gb_s")
         g.close()
     out["cavity129"]["note"] = "config 1: 16 641 nodes, L2-resident, launch-bound; the HBM fraction does not apply"
     return out
@@ -610,6 +613,27 @@ def batch_add(b, L, prob, storage):
     return b.add(*args, open_values=tab, **kw), active
 
 
+def batch_accuracy(L, probs, device, steps=5000, sample=8):
+    """Velocity error of the batched FP32-shifted form against the FP64 path on
+    config 4's own step count: a sample of the problems (alternating cavities
+    and channels, spread over the list) run `steps` steps in an FP32-shifted
+    batch and in an FP64 batch (bit-exact with the reference); relative L2 of
+    u over the active nodes, per problem."""
+    pick = probs[:: max(1, len(probs) // sample)][:sample]
+    us = {}
+    for storage in (L.STORE_F64, L.STORE_F32S):
+        with L.CudaBatch(storage=storage, device=device) as b:
+            slots = [batch_add(b, L, p, storage)[0] for p in pick]
+            b.step(steps - 1)
+            b.synchronize()
+            us[storage] = [b.lattice(s).compute_macro()[1] for s in slots]
+    errs = []
+    for p, u64, u32 in zip(pick, us[L.STORE_F64], us[L.STORE_F32S]):
+        errs.append(float(np.sqrt(((u32 - u64) ** 2).sum() / max((u64 ** 2).sum(), 1e-300))))
+    return {"steps": steps, "problems": [f"{p['kind']} {p['rows']}x{p['cols']}" for p in pick],
+            "u_rel_l2_vs_f64": errs, "max": max(errs), "median": float(np.median(errs))}
+
+
 def run_batch(a, dist):
     """Config 4: 256 uneven problems advanced as one batch (FP32-shifted,
     autotuned launch shape) against each problem alone through the plain FP64
@@ -638,13 +662,14 @@ def run_batch(a, dist):
     sampler.stop()
     batched = dist.world * nodes * a.steps / ms / 1e3
     b.close()
-    # plain FP64 path, one problem at a time, same lattices
-    k_plain = max(1, min(a.steps, 40))
+    # plain FP64 path, one problem at a time, same lattices (100 timed steps
+    # after 20 warm ones per problem, so the sum is stable from box to box)
+    k_plain = 100
     plain_ms = 0.0
     for p in probs:
         g, _ = batch_add(None, L, p, L.STORE_F64)
         g.init()
-        g.step(3)
+        g.step(20)
         g.synchronize()
         g.record(0)
         g.step(k_plain)
@@ -652,6 +677,7 @@ def run_batch(a, dist):
         plain_ms += g.elapsed_ms(0, 1)
         g.close()
     plain = nodes * k_plain / plain_ms / 1e3
+    accuracy = batch_accuracy(L, probs, dist.local) if a.batch_accuracy_steps > 0 else None
     bps = 18 * 4 * active + nodes
     peak = (json.load(open(PEAKS_FILE)).get("hbm_gbs") if os.path.exists(PEAKS_FILE) else None) or FALLBACK_HBM_GBS
     per = ms / a.steps
@@ -668,6 +694,7 @@ def run_batch(a, dist):
         "plain_f64": {"mlups": round(plain, 1), "steps_per_problem": k_plain,
                       "path": "each problem alone through llb_step (FP64, the lattice's default step kernel)"},
         "batched_over_plain_f64": round(batched / plain, 3),
+        "accuracy": accuracy,
         "gpu_launches": (a.steps + spl - 1) // spl, "clocks": sampler.summary(t0, t1),
     }
 
@@ -856,6 +883,8 @@ def main():
                     help="porous workload: skip the batched and served summaries")
     ap.add_argument("--force-steps", type=int, default=50000,
                     help="steps of the config-2 drag/lift comparison of the storage forms (0: skip)")
+    ap.add_argument("--batch-accuracy-steps", type=int, default=5000,
+                    help="batch workload: steps of the FP32-shifted vs FP64 error run on a sample (0: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=20000,
                     help="porous workload: steps of the shifted forms' velocity-error run against FP64")
     a = ap.parse_args()
@@ -916,11 +945,11 @@ def main():
         # the batched and served FP32-shifted forms beside the plain FP64 path
         import copy
         ab = copy.copy(a)
-        ab.steps = min(a.steps, 300)
+        ab.steps = min(max(a.steps, 100), 300)
         bl = run_batch(ab, dist)
         line["batched"] = {"workload": "batch256", "mlups_f32s": bl["value"], "plain_f64_mlups": bl["plain_f64"]["mlups"],
                            "ratio": bl["batched_over_plain_f64"], "roofline_frac": bl["roofline"]["frac"],
-                           "steps": ab.steps, "launch": bl["config"]["launch"]}
+                           "steps": ab.steps, "launch": bl["config"]["launch"], "accuracy": bl["accuracy"]}
         asv = copy.copy(a)
         asv.requests = a.requests
         sl = run_serve(asv, dist)

@@ -277,12 +277,27 @@ int llb_batch_lattice(llb_batch_handle b, int32_t slot, llb_handle* out);
    launch per step, replayed from graphs; >1: cooperative multi-step launches). */
 int llb_batch_set_config(llb_batch_handle b, int32_t block_y, int32_t steps_per_launch);
 int llb_batch_get_config(llb_batch_handle b, int32_t* block_y, int32_t* steps_per_launch);
+/* Which lattices a batch steps on compacted planes (only active nodes stored,
+   one thread per slot) rather than the dense ones: LLB_LAYOUT_AUTO those with
+   at least 5 % of their active nodes next to a wall, obstacle or dead node
+   (the single-lattice default's rule), LLB_LAYOUT_COMPACT every lattice that
+   has them, LLB_LAYOUT_DENSE none.  Attached lattices move at once, at their
+   current step; results do not depend on the layout (FP64 bit for bit). */
+#define LLB_LAYOUT_AUTO 0
+#define LLB_LAYOUT_COMPACT 1
+#define LLB_LAYOUT_DENSE 2
+int llb_batch_set_layout(llb_batch_handle b, int32_t layout);
+int llb_batch_get_layout(llb_batch_handle b, int32_t* layout);
 /* Autotuner: times trial_steps real steps of the batch for every candidate
-   shape (the steps advance the lattices; every candidate computes the same
-   arithmetic) and keeps the fastest. */
+   layout and shape (the steps advance the lattices; every candidate computes
+   the same arithmetic) and keeps the fastest. */
 int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, int32_t* steps_per_launch,
                    float* ms_per_step);
 int llb_batch_get_step(llb_batch_handle b, int64_t* step);
+/* The lattice in `slot` stops before computing step index stop_step: later
+   batch steps leave it as it is (-1: no stop).  A solve server sets each
+   lattice's last step, so chunks need not end at the earliest completion. */
+int llb_batch_set_stop(llb_batch_handle b, int32_t slot, int64_t stop_step);
 /* Waits for the batch; LLB_E_TIMEOUT if a cooperative launch gave up a grid
    barrier.  The lattices' states are then unspecified (blocks that gave up
    skipped their later steps): remove them and add them again.  The barrier
@@ -309,15 +324,17 @@ const char* llb_batch_last_error(llb_batch_handle b);
 /* A request loop over a batch; no counterpart in the reference (one Lattice
    per process, driven by its own main()).  Requests -- a lattice description,
    its boundary values for steps 0..rows-1 and a step count -- are submitted
-   from any thread and queued; they are admitted first come, first served
-   while the device bytes of the admitted lattices fit budget_bytes, and their
-   state stays resident until they finish.  Batched mode: a preparer thread
-   creates admitted lattices while the GPU runs, a worker advances them in two
-   concurrent lanes (lattices under 2^20 nodes in one work-list batch on a
-   high-priority stream, larger ones by their own launches), in chunks of at
-   most max_chunk_steps for the large lane, and a reaper thread copies results
-   and frees.  Sequential mode: one request at a time through the plain
-   single-lattice path.  A request of `steps` steps (>= 2)
+   from any thread and queued; they are admitted while the device bytes of the
+   admitted lattices fit budget_bytes and (batched mode) the resident lattice
+   nodes stay under a cap, shortest work first by default
+   (llb_server_set_admission), and their state stays resident until they
+   finish.  Batched mode: preparer threads create admitted lattices while the
+   GPU runs, a worker advances them in two concurrent batches (lattices under
+   2^20 nodes on a high-priority stream, larger ones on another) in chunks of
+   max_chunk_steps -- each lattice stops on the device at its own last step --
+   and a reaper thread copies results and frees.  Sequential mode: one request
+   at a time, first come first served, through the plain single-lattice path.
+   A request of `steps` steps (>= 2)
    ends with the state the reference's Lattice holds after perform_lbm(steps)
    and returns that call's rho and u: steps - 1 collisions and the macroscopic
    fields of the last step (llb_compute_macro).  The lattice's storage, device
@@ -342,6 +359,16 @@ typedef struct {
 } llb_server_counters;
 int llb_server_create(int32_t device, int32_t storage, int32_t mode, int64_t budget_bytes, int32_t max_chunk_steps,
                       llb_server_handle* out);
+/* Admission policy of the batched mode: at most max_resident_nodes lattice
+   nodes resident at once (0: the default, LLB_SERVE_DEFAULT_NODE_CAP; a
+   request is always admitted when nothing runs), and the order queued
+   requests are admitted in (LLB_ADMIT_SHORTEST_FIRST: least lattice nodes x
+   steps first; LLB_ADMIT_FIFO: oldest first).  The byte budget applies as
+   well. */
+#define LLB_ADMIT_SHORTEST_FIRST 0
+#define LLB_ADMIT_FIFO 1
+#define LLB_SERVE_DEFAULT_NODE_CAP (32LL << 20)
+int llb_server_set_admission(llb_server_handle s, int64_t max_resident_nodes, int32_t order);
 /* Stops the worker after the running requests finish; queued ones fail. */
 int llb_server_destroy(llb_server_handle s);
 /* LLB_E_NOMEM if the lattice alone exceeds the budget.  The description's

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <limits>
 #include <new>
 #include <string>
 #include <vector>
@@ -44,6 +45,7 @@ struct llb_batch {
     unsigned* d_bar = nullptr;           // [count, generation]
     unsigned* d_err = nullptr;
     long long bar_limit = BARRIER_LIMIT;  // polls of the grid barrier before a block gives up
+    int layout = LLB_LAYOUT_AUTO;         // which lattices the batch steps on compacted planes
     int block_y = 4;
     int spl = 1;                         // steps per launch
     bool dirty = true;
@@ -74,27 +76,62 @@ void drop_graph(llb_batch_handle b) {
     }
 }
 
-// Per-lattice step and buffer implied by the batch counter.
+// Batch steps a lattice has taken since it was anchored: the batch's, up to
+// its stop step.
+long long steps_taken(llb_batch_handle b, const BatchLattice& d) {
+    return std::max(0LL, std::min(b->step - d.s0, d.t_end - d.t0));
+}
+
+// Per-lattice step, buffer and state residence implied by the batch counter.
 void sync_handle(llb_batch_handle b, int s) {
     llb_handle h = b->slot[s];
     const BatchLattice& d = b->desc[s];
-    const long long delta = b->step - d.s0;
+    const long long delta = steps_taken(b, d);
     h->step = d.t0 + delta;
     h->cur = d.cur0 ^ static_cast<int>(delta & 1);
+    if (delta > 0) handle_batch_stepped(h, d.compact != 0);
 }
 
 // A lattice stepped through its own handle since the last batch call is
-// re-anchored at its current step and buffer.
-void reanchor_if_moved(llb_batch_handle b, int s) {
+// re-anchored at its current step and buffer, its state brought back into
+// the layout the batch steps.
+int reanchor_if_moved(llb_batch_handle b, int s) {
     llb_handle h = b->slot[s];
     BatchLattice& d = b->desc[s];
-    const long long delta = b->step - d.s0;
+    const long long delta = steps_taken(b, d);
     if (h->step != d.t0 + delta || h->cur != (d.cur0 ^ static_cast<int>(delta & 1))) {
         d.t0 = h->step;
         d.s0 = b->step;
         d.cur0 = h->cur;
         b->dirty = true;
+        if (handle_batch_layout(h, d.compact != 0) != LLB_OK) return bfail(b, LLB_E_CUDA, llb_last_error(h));
     }
+    return LLB_OK;
+}
+
+// Slots of one work-list item of a compacted lattice: one per thread of a block.
+int64_t slots_per_item(const llb_batch_handle b) { return static_cast<int64_t>(BX) * b->block_y; }
+
+// Whether the batch steps this lattice on its compacted planes (building them
+// if needed; a lattice without them runs on the dense ones).
+bool want_compact(llb_batch_handle b, llb_handle h) {
+    if (b->layout == LLB_LAYOUT_DENSE) return false;
+    if (b->layout == LLB_LAYOUT_AUTO && !obstacle_rich(*h)) return false;
+    return handle_prepare_compact(h) == LLB_OK;
+}
+
+// Descriptor fields that follow the lattice's layout and position.
+void anchor(llb_batch_handle b, int s, bool compact) {
+    llb_handle h = b->slot[s];
+    BatchLattice& d = b->desc[s];
+    d.compact = compact ? 1 : 0;
+    d.f[0] = compact ? h->cf[0] : h->f[0];
+    d.f[1] = compact ? h->cf[1] : h->f[1];
+    d.cg = compact ? handle_compact_geo(h) : CompactGeo{};
+    d.t0 = h->step;
+    d.s0 = b->step;
+    d.cur0 = h->cur;
+    b->dirty = true;
 }
 
 int rebuild(llb_batch_handle b) {
@@ -108,11 +145,17 @@ int rebuild(llb_batch_handle b) {
         const int idx = static_cast<int>(dev.size());
         b->order.push_back(s);
         dev.push_back(b->desc[s]);
-        // every lattice, large or small, is tiles of the one work list: one
+        // every lattice, large or small, is items of the one work list: one
         // persistent launch advances the whole batch
         const BatchLattice& d = b->desc[s];
-        const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
-        for (int t = 0; t < d.nti * ntj; ++t) items.push_back(make_int2(idx, t));
+        int64_t n;
+        if (d.compact) {
+            n = (d.cg.n_slots + slots_per_item(b) - 1) / slots_per_item(b);
+        } else {
+            const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
+            n = static_cast<int64_t>(d.nti) * ntj;
+        }
+        for (int64_t t = 0; t < n; ++t) items.push_back(make_int2(idx, static_cast<int>(t)));
     }
     LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
     if (static_cast<int>(dev.size()) > b->desc_cap) {
@@ -292,29 +335,37 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
     if (!h->own_stream) return bfail(b, LLB_E_STATE, "lattice already belongs to a batch");
     if (h->d_ps) return bfail(b, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the single-lattice path");
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
-    // the batch's kernels step the dense planes
-    if (handle_leave_compact(h) != LLB_OK) return bfail(b, LLB_E_CUDA, llb_last_error(h));
+    // the batch steps the compacted planes (built here, on the lattice's own
+    // stream, so a chunk running on the batch's stream is not waited for);
+    // lattices without them run on the dense ones
+    const bool compact = want_compact(b, h);
+    if (!compact && handle_leave_compact(h) != LLB_OK) return bfail(b, LLB_E_CUDA, llb_last_error(h));
     // the lattice works on the batch's stream from now on
     LLB_BCUDA(b, cudaStreamSynchronize(h->stream));
     cudaStreamDestroy(h->stream);
     h->stream = b->stream;
     h->own_stream = false;
+    // on failure the handle gets a stream of its own again so the caller can destroy it
+    auto give_back = [&](int rc, const std::string& why) {
+        cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        h->own_stream = true;
+        return bfail(b, rc, why);
+    };
     if (!h->initialized) {
         const int rc = llb_init(h, 0);
-        if (rc != LLB_OK) {
-            // give the handle a stream of its own again so the caller can destroy it
-            cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-            h->own_stream = true;
-            return bfail(b, rc, "llb_init failed");
-        }
+        if (rc != LLB_OK) return give_back(rc, "llb_init failed");
     }
+    if (handle_batch_layout(h, compact) != LLB_OK) return give_back(LLB_E_CUDA, llb_last_error(h));
     BatchLattice d{};
     const LaunchCtx x = handle_ctx(h);
     d.g = x.g;
     d.ot = x.ot;
     d.c = x.c;
-    d.f[0] = h->f[0];
-    d.f[1] = h->f[1];
+    d.compact = compact ? 1 : 0;
+    d.f[0] = compact ? h->cf[0] : h->f[0];
+    d.f[1] = compact ? h->cf[1] : h->f[1];
+    if (compact) d.cg = handle_compact_geo(h);
+    d.t_end = std::numeric_limits<long long>::max();
     d.t0 = h->step;
     d.s0 = b->step;
     d.cur0 = h->cur;
@@ -371,9 +422,10 @@ int llb_batch_remove(llb_batch_handle b, int32_t slot) {
 int llb_batch_step(llb_batch_handle b, int32_t nsteps) {
     if (!b || nsteps < 0) return LLB_E_INVALID;
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    int rc = LLB_OK;
     for (int s = 0; s < static_cast<int>(b->slot.size()); ++s)
-        if (b->slot[s]) reanchor_if_moved(b, s);
-    int rc = rebuild(b);
+        if (b->slot[s] && (rc = reanchor_if_moved(b, s)) != LLB_OK) return rc;
+    rc = rebuild(b);
     if (rc != LLB_OK) return rc;
     if ((rc = launch_steps(b, nsteps)) != LLB_OK) return rc;
     for (int s = 0; s < static_cast<int>(b->slot.size()); ++s)
@@ -411,13 +463,17 @@ int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, in
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
     static const int shapes[] = {1, 2, 4, 8};
     static const int spls[] = {1, 8};
+    static const int layouts[] = {LLB_LAYOUT_AUTO, LLB_LAYOUT_COMPACT, LLB_LAYOUT_DENSE};
     float best = 1e30f;
-    int best_by = b->block_y, best_spl = b->spl;
+    int best_by = b->block_y, best_spl = b->spl, best_layout = b->layout;
     for (int e = 0; e < 2; ++e)
         if (!b->ev[e]) LLB_BCUDA(b, cudaEventCreate(&b->ev[e]));
-    for (int by : shapes) {
+    for (int layout : layouts) {
+      int rc = llb_batch_set_layout(b, layout);
+      if (rc != LLB_OK) return rc;
+      for (int by : shapes) {
         for (int spl : spls) {
-            int rc = llb_batch_set_config(b, by, spl);
+            rc = llb_batch_set_config(b, by, spl);
             if (rc != LLB_OK) return rc;
             if ((rc = llb_batch_step(b, std::min(trial_steps, 8))) != LLB_OK) return rc;  // graph capture, warm-up
             LLB_BCUDA(b, cudaEventRecord(b->ev[0], b->stream));
@@ -430,10 +486,13 @@ int llb_batch_tune(llb_batch_handle b, int32_t trial_steps, int32_t* block_y, in
                 best = ms;
                 best_by = by;
                 best_spl = spl;
+                best_layout = layout;
             }
         }
+      }
     }
-    int rc = llb_batch_set_config(b, best_by, best_spl);
+    int rc = llb_batch_set_layout(b, best_layout);
+    if (rc == LLB_OK) rc = llb_batch_set_config(b, best_by, best_spl);
     if (rc != LLB_OK) return rc;
     if (block_y) *block_y = best_by;
     if (steps_per_launch) *steps_per_launch = best_spl;
@@ -476,6 +535,45 @@ int llb_batch_synchronize(llb_batch_handle b) {
         LLB_BCUDA(b, cudaMemset(b->d_err, 0, sizeof(unsigned)));
         return bfail(b, LLB_E_TIMEOUT, "batched kernel gave up a grid barrier");
     }
+    return LLB_OK;
+}
+
+int llb_batch_set_layout(llb_batch_handle b, int32_t layout) {
+    if (!b || layout < LLB_LAYOUT_AUTO || layout > LLB_LAYOUT_DENSE) return LLB_E_INVALID;
+    if (layout == b->layout) return LLB_OK;
+    if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
+    b->layout = layout;
+    // every attached lattice moves into the layout it now takes, at its current step
+    for (int s = 0; s < static_cast<int>(b->slot.size()); ++s) {
+        llb_handle h = b->slot[s];
+        if (!h) continue;
+        sync_handle(b, s);
+        const bool compact = want_compact(b, h);
+        if (handle_batch_layout(h, compact) != LLB_OK) return bfail(b, LLB_E_CUDA, llb_last_error(h));
+        anchor(b, s, compact);
+    }
+    drop_graph(b);
+    return LLB_OK;
+}
+
+int llb_batch_get_layout(llb_batch_handle b, int32_t* layout) {
+    if (!b || !layout) return LLB_E_INVALID;
+    *layout = b->layout;
+    return LLB_OK;
+}
+
+int llb_batch_set_stop(llb_batch_handle b, int32_t slot, int64_t stop_step) {
+    if (!b || slot < 0 || slot >= static_cast<int>(b->slot.size()) || !b->slot[slot] || stop_step < -1)
+        return LLB_E_INVALID;
+    BatchLattice& d = b->desc[slot];
+    // re-anchor at the lattice's current position, then set the stop
+    sync_handle(b, slot);
+    llb_handle h = b->slot[slot];
+    d.t0 = h->step;
+    d.s0 = b->step;
+    d.cur0 = h->cur;
+    d.t_end = stop_step < 0 ? std::numeric_limits<long long>::max() : std::max<long long>(stop_step, h->step);
+    b->dirty = true;
     return LLB_OK;
 }
 

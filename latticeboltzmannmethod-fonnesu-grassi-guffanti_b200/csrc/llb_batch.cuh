@@ -2,9 +2,12 @@
 // advanced by one persistent launch.
 //
 // Every lattice is described by a BatchLattice in device memory; the work list
-// holds one item per (lattice, tile of 32 rows x blockDim.y columns).  A
-// persistent grid walks the items with a grid-stride loop, so lattices of any
-// size share the launch and the load balances at tile granularity.  A lattice
+// holds one item per (lattice, block of slots) for lattices on compacted
+// planes (llb_compact.cuh: only active nodes, every lane busy) and per
+// (lattice, tile of 32 rows x blockDim.y columns) for lattices on dense
+// planes.  A persistent grid walks the items with a grid-stride loop, so
+// lattices of any size share the launch and the load balances at item
+// granularity.  A lattice
 // joins the batch at batch step s0 with its step index t0 and current buffer
 // cur0; at batch step s it is at step t0 + (s - s0) and reads buffer
 // cur0 ^ ((s - s0) & 1), so lattices that joined at different times coexist and
@@ -16,7 +19,7 @@
 // the kernel returns.
 #pragma once
 
-#include "llb_kernels.cuh"
+#include "llb_compact.cuh"
 
 namespace llb {
 
@@ -24,12 +27,15 @@ struct BatchLattice {
     Geometry g;
     OpenTable ot;
     Collision c;
-    void* f[2];
+    void* f[2];     // the planes the batch steps: dense, or compacted when `compact`
     long long t0;   // lattice step index at batch step s0
     long long s0;
+    long long t_end;  // the lattice stops before step index t_end (later batch steps leave it as it is)
     int cur0;       // buffer holding the lattice's state at batch step s0
     int nti;        // row tiles: ceil(rows / 32)
+    int compact;    // 1: compacted planes (cg), items are blocks of slots
     unsigned* flags;
+    CompactGeo cg;
 };
 
 constexpr long long BARRIER_LIMIT = 1LL << 22;
@@ -73,6 +79,7 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     const long long d = s - Lp->s0;
     const int cur = Lp->cur0 ^ static_cast<int>(d & 1);
     const long long t = Lp->t0 + d;
+    if (t >= Lp->t_end) return;  // block-uniform: the lattice has finished
     const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
     T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
     const Geometry g = Lp->g;
@@ -112,6 +119,24 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
 }
 
+// One item of a compacted lattice: (threads of the block) consecutive slots.
+template <class M>
+__device__ __forceinline__ void batch_slots(const BatchLattice* __restrict__ Lp, int item, long long s) {
+    using T = typename M::T;
+    const long long d = s - Lp->s0;
+    const long long t = Lp->t0 + d;
+    if (t >= Lp->t_end) return;  // block-uniform: the lattice has finished
+    const int cur = Lp->cur0 ^ static_cast<int>(d & 1);
+    const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
+    T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
+    const int nthr = blockDim.x * blockDim.y;
+    const long long slot = static_cast<long long>(item) * nthr + threadIdx.y * blockDim.x + threadIdx.x;
+    // the descriptor's fields are read where they are used (L1-resident), not
+    // copied into registers
+    const bool bad = compact_slot<M, -1>(Lp->g, Lp->cg, Lp->ot, Lp->c, fin, fout, t, slot);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(Lp->flags, 1u);
+}
+
 // One launch: `steps` batch steps starting at batch step (*sbase + soff).
 template <class M>
 __global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __restrict__ lats,
@@ -126,7 +151,8 @@ __global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __
         for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
             const int nxt = item + gridDim.x;
             const int2 it_next = nxt < n_items ? items[nxt] : it;
-            batch_tile<M>(lats + it.x, it.y, s);
+            if (lats[it.x].compact) batch_slots<M>(lats + it.x, it.y, s);
+            else batch_tile<M>(lats + it.x, it.y, s);
             it = it_next;
         }
         if (st + 1 < steps && !grid_barrier(bar, bar + 1, gridDim.x, bar_limit)) {

@@ -618,6 +618,21 @@ int handle_force_context(llb_handle h, LaunchCtx* ctx, const void** fin, double*
 int handle_fail(llb_handle h, int code, const char* msg) { return fail(h, code, msg); }
 LaunchCtx handle_ctx(llb_handle h) { return make_ctx(h); }
 int handle_dense_state(llb_handle h) { return state_to_dense(h); }
+int handle_prepare_compact(llb_handle h) {
+    int rc = select_device(h);
+    if (rc) return rc;
+    if (h->d_ps) return LLB_E_UNSUPPORTED;
+    rc = build_compact(h);
+    if (rc != LLB_OK) h->err.clear();
+    return rc;
+}
+int handle_batch_layout(llb_handle h, bool compact) {
+    int rc = select_device(h);
+    if (rc) return rc;
+    return compact ? state_to_compact(h) : state_to_dense(h);
+}
+void handle_batch_stepped(llb_handle h, bool compact) { h->where = compact ? RES_COMPACT : RES_DENSE; }
+CompactGeo handle_compact_geo(llb_handle h) { return compact_geo(h); }
 int handle_leave_compact(llb_handle h) {
     int rc = select_device(h);
     if (rc) return rc;

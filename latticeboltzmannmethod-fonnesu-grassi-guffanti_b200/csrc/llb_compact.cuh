@@ -99,14 +99,20 @@ __device__ __forceinline__ void pull_compact_general(const Geometry& g, const Co
     }
 }
 
-// One plain step (steps 1-4 of llb_kernels.cuh) over the compacted planes: one
-// thread per slot; padding slots store the initial values, so every 32-byte
-// sector of a column's run is written whole.
+// One slot of a step (steps 1-4 of llb_kernels.cuh) over the compacted planes:
+// pull, closure, moments, collision, store.  Padding slots store the initial
+// values, so every 32-byte sector of a column's run is written whole.  Every
+// lane of the warp calls it (warp vote inside).  Returns whether a non-finite
+// density was seen.  COLL: 0 BGK, 1 TRT, -1 the lattice's own (c.model; a
+// batch holds both).
+//
+// One slot per thread: a variant that gave each thread 2 (FP32) or 4 (FP16)
+// slots with all their loads issued first ran slower on B200 in every form
+// (porous 4096^2: FP16 103.7k -> 77.7k, FP32 98.3k -> 93.1k MLUPS).
 template <class M, int COLL>
-__global__ void __launch_bounds__(COMPACT_BLOCK, 5) k_step_compact(Geometry g, CompactGeo cg, OpenTable ot,
-                                                                   Collision c, const typename M::T* __restrict__ fin,
-                                                                   typename M::T* __restrict__ fout, StepSync ss) {
-    const long long t = static_cast<long long>(blockIdx.x) * COMPACT_BLOCK + threadIdx.x;
+__device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo& cg, const OpenTable& ot,
+                                             const Collision& c, const typename M::T* __restrict__ fin,
+                                             typename M::T* __restrict__ fout, long long tstep, long long t) {
     const bool in = t < cg.n_slots;
     unsigned info = 0, nb = 0;
     if (in) {
@@ -156,7 +162,7 @@ __global__ void __launch_bounds__(COMPACT_BLOCK, 5) k_step_compact(Geometry g, C
         typename M::R rr, xr, yr;
         if (cls == CLS_OPEN) {
             double rho, ux, uy;
-            open_node<M>(ot, g.open_idx[nb], m, current_step(ss), f, rho, ux, uy);
+            open_node<M>(ot, g.open_idx[nb], m, tstep, f, rho, ux, uy);
             rr = M::from_f64(rho);
             xr = static_cast<typename M::R>(ux);
             yr = static_cast<typename M::R>(uy);
@@ -164,13 +170,24 @@ __global__ void __launch_bounds__(COMPACT_BLOCK, 5) k_step_compact(Geometry g, C
             M::moments(f, rr, xr, yr);
             bad = !M::finite(rr);
         }
-        M::template collide<COLL>(f, rr, xr, yr, c);
+        if (COLL == 0 || (COLL < 0 && c.model == 0)) M::template collide<0>(f, rr, xr, yr, c);
+        else M::template collide<1>(f, rr, xr, yr, c);
 #pragma unroll
         for (int k = 0; k < 9; ++k) M::store(fout + k * P + t, f[k]);
     } else if (in) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) M::store(fout + k * P + t, M::keep(k));
     }
+    return bad;
+}
+
+// One plain step over the compacted planes: one thread per slot.
+template <class M, int COLL>
+__global__ void __launch_bounds__(COMPACT_BLOCK, 5) k_step_compact(Geometry g, CompactGeo cg, OpenTable ot,
+                                                                   Collision c, const typename M::T* __restrict__ fin,
+                                                                   typename M::T* __restrict__ fout, StepSync ss) {
+    const long long t = static_cast<long long>(blockIdx.x) * COMPACT_BLOCK + threadIdx.x;
+    const bool bad = compact_slot<M, COLL>(g, cg, ot, c, fin, fout, current_step(ss), t);
     flag_numerics(ss, bad);
 }
 

@@ -92,23 +92,28 @@ struct llb_lattice {
 constexpr int RES_DENSE = 0, RES_COMPACT = 1, RES_BOTH = 2;
 
 // Default plain-step kernel of a lattice, from measurements on B200 (cavities,
-// channels, cylinders and porous media from 724^2 to 4096^2, every storage
+// channels, cylinders and porous media from 256^2 to 4096^2, every storage
 // form):
-//  * below 2^19 nodes: one thread per node;
-//  * at least 5 % of the active nodes not PLAIN (porous media): the TMA
-//    pipeline -- FP64 configuration 1 from 2^21 nodes, else 0; configuration
-//    6 for the shifted forms (configuration 0 plus the tile's bounce bytes);
-//    its bounce-back is a shared-memory address select, and its tiles stage
-//    every node;
-//  * open flow whose resident state (two buffers of 9 planes) exceeds the L2
-//    cache several times over: two steps per pass for FP64 and FP32
-//    (configuration 3, from 2^28 bytes), the TMA pipeline for FP16 (from 2^27
-//    bytes);
-//  * otherwise one thread per node, which reads only active sectors and runs
-//    close to the copy bandwidth on open flow.
+//  * at least 5 % of the active nodes not PLAIN (porous media) and at least
+//    2^18 nodes: the compacted planes (only active nodes stored and read; on
+//    porous 4096^2 FP64 63.1k MLUPS against 46.8k for the best dense kernel,
+//    which also pulls the obstacle interiors through DRAM);
+//  * otherwise the dense kernels: below 2^19 nodes one thread per node; open
+//    flow whose resident state (two buffers of 9 planes) exceeds the L2 cache
+//    several times over: two steps per pass for FP64 and FP32 (configuration
+//    3, from 2^28 bytes), the TMA pipeline for FP16 (from 2^27 bytes); else
+//    one thread per node, which runs close to the copy bandwidth on open flow
+//    (there every node is active and the compacted planes only add their
+//    6 bytes of addressing per node).
 constexpr int PIPE_GRID = -1, PIPE_LIST = -2, PIPE_COMPACT = -3;
 constexpr int64_t TMA_MIN_NODES = 1 << 19;
 constexpr double TMA_MIN_NONPLAIN = 0.05;
+constexpr int64_t COMPACT_MIN_NODES = 1 << 18;
+inline bool obstacle_rich(const llb_lattice& h) {
+    return h.n_active > 0 &&
+           static_cast<double>(h.n_nonplain) >= TMA_MIN_NONPLAIN * static_cast<double>(h.n_active);
+}
+// The best dense kernel (also the choice for lattices without compacted planes).
 inline int default_dense_pipeline(const llb_lattice& h) {
     const int64_t n = h.R * h.C;
     if (n < TMA_MIN_NODES || h.n_active == 0) return PIPE_GRID;
@@ -118,7 +123,10 @@ inline int default_dense_pipeline(const llb_lattice& h) {
     if (h.storage == LLB_STORE_F16S) return state >= static_cast<double>(int64_t{1} << 27) ? 0 : PIPE_GRID;
     return state >= static_cast<double>(int64_t{1} << 28) ? llb::FIRST_PAIR_CONFIG : PIPE_GRID;
 }
-inline int default_pipeline(const llb_lattice& h) { return default_dense_pipeline(h); }
+inline int default_pipeline(const llb_lattice& h) {
+    if (obstacle_rich(h) && h.R * h.C >= COMPACT_MIN_NODES) return PIPE_COMPACT;
+    return default_dense_pipeline(h);
+}
 
 namespace llb {
 // Launch context of a handle's current state (defined in llb_capi.cu).
@@ -131,4 +139,15 @@ int handle_dense_state(llb_handle h);
 // Before a batch takes a handle: its state in the dense planes, and a handle
 // on the compacted pipeline moves to the one-thread-per-node kernel.
 int handle_leave_compact(llb_handle h);
+// The compacted planes and tables of a handle (built once; host work and a
+// synchronisation of the handle's stream).  LLB_OK, or an error when the
+// lattice has none (partially saturated obstacles, too large).
+int handle_prepare_compact(llb_handle h);
+// The state of a handle moved into the layout a batch steps (a copy kernel on
+// the handle's stream when needed).
+int handle_batch_layout(llb_handle h, bool compact);
+// A batch has stepped the handle's lattice in that layout.
+void handle_batch_stepped(llb_handle h, bool compact);
+// Addressing tables of the handle's compacted planes (after handle_prepare_compact).
+CompactGeo handle_compact_geo(llb_handle h);
 }  // namespace llb

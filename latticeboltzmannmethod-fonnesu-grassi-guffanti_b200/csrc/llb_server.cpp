@@ -2,15 +2,19 @@
 // values and a step count -- arrive from any thread and are served by native
 // threads that keep every admitted lattice resident on the device.
 //
-// Batched mode (continuous batching) runs three threads:
-//  * preparer threads admit queued requests first come, first served while
-//    their device memory fits the budget, and create each lattice (mask build,
-//    allocation, upload) on a stream of its own, several at a time;
+// Batched mode (continuous batching) runs three kinds of threads:
+//  * preparer threads admit queued requests -- shortest work first (lattice
+//    nodes x steps) by default, or first come, first served -- while their
+//    device memory fits the budget and the resident lattice nodes stay under
+//    a cap (enough nodes to keep HBM busy; more only stretches every
+//    request's time on the device), and create each lattice (mask build,
+//    compacted planes, allocation, upload) on a stream of its own, several at
+//    a time;
 //  * the worker moves prepared lattices into one of two lanes, each a batch on
-//    its own stream -- lattices of fewer than 2^20 nodes share the work-list
-//    kernel (small lane), larger ones are stepped by their own launches (large
-//    lane) -- and advances each lane chunk by chunk, at most max_chunk steps
-//    and never past the lane's earliest completion.  The lanes run
+//    its own stream (lattices of fewer than 2^20 nodes in the small lane), and
+//    advances each lane chunk by chunk, max_chunk steps at a time: a lattice
+//    carries its own stop step, so one that finishes inside a chunk stops
+//    there on the device while the others run on.  The lanes run
 //    concurrently and independently: a lane whose chunk is done is drained
 //    and relaunched at once while the other runs on.  The small lane's stream
 //    has the higher scheduling priority, so a small request keeps its own step
@@ -64,6 +68,7 @@ struct Request {
     double t_submit = 0, t_admit = 0, t_done = 0;
     llb_handle h = nullptr;     // the lattice while it is prepared, running or retired
     int rc = LLB_OK;            // outcome of its steps
+    bool counted_nodes = false;  // its nodes count against the resident-node cap
     std::vector<double> rho, u;
     std::string error;
 };
@@ -88,6 +93,9 @@ struct llb_server {
     int mode = LLB_SERVE_BATCHED;
     int64_t budget = 0;
     int32_t max_chunk = 256;
+    int64_t node_cap = LLB_SERVE_DEFAULT_NODE_CAP;  // resident lattice nodes, at most (batched mode)
+    int order = LLB_ADMIT_SHORTEST_FIRST;
+    int64_t resident_nodes = 0;
     llb_batch_handle batch[2] = {nullptr, nullptr};  // small lane, large lane
     std::mutex mu;
     std::condition_variable cv_prep;   // the preparer: queued requests, freed bytes, stop
@@ -135,6 +143,7 @@ void complete(llb_server_handle s, const std::shared_ptr<Request>& r, int rc, co
     }
     s->in_use -= r->bytes;
     s->admitted -= 1;
+    if (r->counted_nodes) s->resident_nodes -= r->desc.rows * r->desc.cols;
     s->cv_done.notify_all();
     s->cv_prep.notify_all();
 }
@@ -194,15 +203,30 @@ constexpr int64_t LARGE_LANE_NODES = 1 << 20;
 
 int lane_of(const Request& r) { return r.desc.rows * r.desc.cols >= LARGE_LANE_NODES ? 1 : 0; }
 
+// The queued request admitted next (shortest work first, or the oldest), if
+// it fits the budget and the resident-node cap; queue.end() otherwise.  A
+// request is always admitted when nothing else runs.  Called with s->mu held.
+std::deque<std::shared_ptr<Request>>::iterator next_admission(llb_server_handle s) {
+    auto pick = s->queue.begin();
+    if (pick == s->queue.end()) return pick;
+    if (s->order == LLB_ADMIT_SHORTEST_FIRST) {
+        auto work = [](const Request& r) { return r.desc.rows * r.desc.cols * r.steps; };
+        for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
+            if (work(**it) < work(**pick)) pick = it;
+    }
+    const Request& r = **pick;
+    if (s->admitted == 0) return pick;
+    if (s->in_use + r.bytes > s->budget) return s->queue.end();
+    if (s->resident_nodes + r.desc.rows * r.desc.cols > s->node_cap) return s->queue.end();
+    return pick;
+}
+
 void preparer_loop(llb_server_handle s) {
     for (;;) {
         std::shared_ptr<Request> r;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_prep.wait(lk, [&] {
-                return s->stop ||
-                       (!s->queue.empty() && (s->in_use + s->queue.front()->bytes <= s->budget || s->admitted == 0));
-            });
+            s->cv_prep.wait(lk, [&] { return s->stop || next_admission(s) != s->queue.end(); });
             if (s->stop) {
                 if (--s->preparers_live == 0) {
                     s->preparer_done = true;
@@ -210,17 +234,22 @@ void preparer_loop(llb_server_handle s) {
                 }
                 return;
             }
-            r = s->queue.front();
-            s->queue.pop_front();
+            auto it = next_admission(s);
+            r = *it;
+            s->queue.erase(it);
             r->state = LLB_REQ_RUNNING;
             r->t_admit = now_s();
             s->in_use += r->bytes;
             s->admitted += 1;
+            s->resident_nodes += r->desc.rows * r->desc.cols;
+            r->counted_nodes = true;
         }
         const double t0 = now_s();
         llb_desc d = r->desc;
         int rc = llb_create(&d, &r->h);
         if (rc == LLB_OK && r->rows > 0) rc = llb_set_open_values(r->h, 0, r->rows, r->values.data());
+        // the compacted planes the batch steps, built here rather than on the worker's path
+        if (rc == LLB_OK) llb_set_pipeline(r->h, -3);
         if (rc == LLB_OK) rc = llb_synchronize(r->h);
         int64_t actual = 0;
         if (rc == LLB_OK) rc = llb_device_bytes(r->h, &actual);
@@ -284,13 +313,16 @@ void drain_lane(llb_server_handle s, int ln) {
     s->wait_s += now_s() - t0;
 }
 
-// Next chunk of a lane: at most max_chunk steps, never past its earliest completion.
+// Next chunk of a lane: max_chunk steps, or fewer when every running lattice
+// finishes sooner; a lattice that finishes inside the chunk stops at its own
+// stop step on the device.
 void launch_lane(llb_server_handle s, int ln) {
     llb_batch_handle b = s->batch[ln];
-    int64_t n = s->max_chunk;
-    for (auto& r : s->running[ln]) n = std::min(n, r->remaining);
+    int64_t n = 0;
+    for (auto& r : s->running[ln]) n = std::max(n, r->remaining);
+    n = std::min<int64_t>(n, s->max_chunk);
     const int rc = llb_batch_step(b, static_cast<int32_t>(n));
-    for (auto& r : s->running[ln]) r->remaining -= n;
+    for (auto& r : s->running[ln]) r->remaining -= std::min(n, r->remaining);
     std::lock_guard<std::mutex> lk(s->mu);
     if (rc != LLB_OK) {
         // every running request of the lane fails at its next drain
@@ -333,6 +365,11 @@ void batched_loop(llb_server_handle s) {
             }
             r->slot = slot;
             r->remaining = r->steps - 2;  // step 0 was the first collision
+            // the lattice stops on the device after its last step, whatever the chunk
+            llb_handle view = nullptr;
+            int64_t t_now = 0;
+            if (llb_batch_lattice(s->batch[ln], slot, &view) == LLB_OK && llb_get_step(view, &t_now) == LLB_OK)
+                llb_batch_set_stop(s->batch[ln], slot, t_now + r->remaining);
             s->running[ln].push_back(r);
         }
         // 2. every lane whose chunk is done (or that has none): drain, relaunch
@@ -425,6 +462,16 @@ int llb_server_create(int32_t device, int32_t storage, int32_t mode, int64_t bud
         return drop(LLB_E_NOMEM);
     }
     *out = s;
+    return LLB_OK;
+}
+
+int llb_server_set_admission(llb_server_handle s, int64_t max_resident_nodes, int32_t order) {
+    if (!s || max_resident_nodes < 0 || (order != LLB_ADMIT_SHORTEST_FIRST && order != LLB_ADMIT_FIFO))
+        return LLB_E_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->node_cap = max_resident_nodes == 0 ? LLB_SERVE_DEFAULT_NODE_CAP : max_resident_nodes;
+    s->order = order;
+    s->cv_prep.notify_all();
     return LLB_OK;
 }
 

@@ -32,10 +32,13 @@
 #include <llalbm_cuda.h>
 
 #include <algorithm>
+#include <bitset>
 #include <chrono>
+#include <fstream>
 #include <cstdlib>
 #include <iostream>
 #include <map>
+#include <sstream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -123,6 +126,102 @@ namespace llalbm::core
         {
             if (rc != LLB_OK)
                 throw std::runtime_error(std::string("CUDAPolicy: ") + what + ": " + llb_writer_last_error(w));
+        }
+
+        /**
+         * The reference's lattice-file reader, read_lattice_file<2>
+         * (utils/readers/LatticeReader.hpp:367-522), with its classification --
+         * the per-node std::find scans of identify_obstacle_propagation
+         * (utils/analysis/NodeIdentification.hpp:137-211), O(N^2) -- replaced by
+         * the library's O(R*C) one (llb_classify_*, the same rules).  Same file
+         * format and header checks (dimensions 2, positive extents, per-type
+         * counts summing to R*C, one `i j type` line per non-fluid node), and the
+         * same node vectors in the same order: fluid, boundary (type NONE),
+         * inlet and outlet (their side), wet obstacles (their direction bits).
+         * Where the reference asserts, this throws std::runtime_error; a header
+         * count that differs from the nodes listed also throws (the reference's
+         * vectors would keep default entries or overflow their .at()).
+         */
+        inline void read_lattice_file_fast(const std::string& path, std::vector<Point<2>>& fluid,
+                                           std::vector<BoundaryPoint<2>>& boundary,
+                                           std::vector<BoundaryPoint<2>>& inlet, std::vector<BoundaryPoint<2>>& outlet,
+                                           std::vector<ObstaclePoint<2>>& obstacle,
+                                           std::array<Eigen::Index, 2>& dims)
+        {
+            std::ifstream in(path);
+            if (!in.is_open()) throw std::runtime_error("lattice file could not be opened: " + path);
+            auto bad = [&](const std::string& why) { return std::runtime_error("lattice file " + path + ": " + why); };
+            auto numbers = [&](std::vector<long long>& v) {
+                std::string line;
+                if (!std::getline(in, line)) throw bad("header ends early");
+                std::istringstream ss(line);
+                long long x;
+                v.clear();
+                while (ss >> x) v.push_back(x);
+            };
+            std::vector<long long> h;
+            numbers(h);
+            if (h.size() != 1 || h[0] != 2) throw bad("file and template dimensions do not match");
+            numbers(h);
+            if (h.size() != 2 || h[0] <= 0 || h[1] <= 0) throw bad("extensions must be two positive numbers");
+            const long long R = h[0], C = h[1];
+            std::vector<long long> counts;
+            numbers(counts);
+            long long total = 0;
+            for (long long c : counts) {
+                if (c < 0) throw bad("negative node count");
+                total += c;
+            }
+            if (counts.size() < 6 || total != R * C) throw bad("node counts do not add up to the lattice size");
+            // InputNodeType codes (utils/aliases.hpp): FLUID 0, SOLID 1, BOUNDARY 2, INLET 3, OUTLET 4, OBSTACLE 5
+            std::vector<uint8_t> types(static_cast<std::size_t>(R * C), LLB_NODE_FLUID);
+            // the file lists the non-fluid nodes; every other node is fluid
+            const long long listed = total - counts[0];
+            long long tally[6] = {R * C - listed, 0, 0, 0, 0, 0};
+            for (long long q = 0; q < listed; ++q) {
+                long long i, j, t;
+                if (!(in >> i >> j >> t)) throw bad("fewer node lines than the header announces");
+                if (i < 0 || j < 0 || i >= R || j >= C || t < 0 || t > 5) throw bad("node line out of range");
+                uint8_t& cell = types[static_cast<std::size_t>(i + R * j)];
+                if (cell != LLB_NODE_FLUID) throw bad("node listed twice");
+                cell = static_cast<uint8_t>(t);
+                ++tally[t];
+            }
+            for (int t = 0; t < 6; ++t)
+                if (tally[t] != counts[static_cast<std::size_t>(t)]) throw bad("header counts differ from the nodes listed");
+            int64_t n[5];
+            if (llb_classify_count(R, C, types.data(), n) != LLB_OK)
+                throw bad("an inlet or outlet node lies off the lattice perimeter");
+            std::vector<int64_t> fij(2 * n[0]), wij(2 * n[1]), iij(2 * n[2]), oij(2 * n[3]), bij(2 * n[4]);
+            std::vector<int32_t> iside(n[2]), oside(n[3]);
+            std::vector<uint16_t> dirs(n[4]);
+            llb_node_lists L{n[0], n[1], n[2], n[3], n[4], fij.data(), wij.data(), iij.data(), iside.data(),
+                             oij.data(), oside.data(), bij.data(), dirs.data()};
+            if (llb_classify_fill(R, C, types.data(), &L) != LLB_OK) throw bad("classification failed");
+            dims = {static_cast<Eigen::Index>(R), static_cast<Eigen::Index>(C)};
+            fluid.resize(static_cast<std::size_t>(n[0]));
+            for (int64_t q = 0; q < n[0]; ++q) {
+                fluid[q].coords[0] = fij[2 * q];
+                fluid[q].coords[1] = fij[2 * q + 1];
+            }
+            auto fill_boundary = [](std::vector<BoundaryPoint<2>>& v, const std::vector<int64_t>& ij,
+                                    const int32_t* side, int64_t m) {
+                v.resize(static_cast<std::size_t>(m));
+                for (int64_t q = 0; q < m; ++q) {
+                    v[q].coords[0] = ij[2 * q];
+                    v[q].coords[1] = ij[2 * q + 1];
+                    v[q].type = side ? static_cast<btypes>(side[q]) : btypes::NONE;
+                }
+            };
+            fill_boundary(boundary, wij, nullptr, n[1]);
+            fill_boundary(inlet, iij, iside.data(), n[2]);
+            fill_boundary(outlet, oij, oside.data(), n[3]);
+            obstacle.resize(static_cast<std::size_t>(n[4]));
+            for (int64_t q = 0; q < n[4]; ++q) {
+                obstacle[q].coords[0] = bij[2 * q];
+                obstacle[q].coords[1] = bij[2 * q + 1];
+                obstacle[q].directions = std::bitset<9>(dirs[q]);
+            }
         }
     }  // namespace cuda_detail
 
@@ -386,8 +485,8 @@ namespace llalbm::core
         Lattice(const std::string& path_, const std::size_t& q_, std::ostream& out_stream = std::cout)
             : q(q_), logger("LATTICE", out_stream)
         {
-            llalbm::util::reader::read_lattice_file(path_, fluid_nodes, boundary_coord, inlet_nodes_coord,
-                                                    outlet_nodes_coord, obstacle_nodes, lattice_dimensions);
+            cuda_detail::read_lattice_file_fast(path_, fluid_nodes, boundary_coord, inlet_nodes_coord,
+                                                outlet_nodes_coord, obstacle_nodes, lattice_dimensions);
             logger.info("Constructing CUDA Lattice Object...");
             build_tensors();
             Policy::attach_nodes(inlet_nodes_coord, outlet_nodes_coord);

@@ -31,6 +31,8 @@ BC_ZH_VELOCITY, BC_OPEN, BC_ZH_PRESSURE = 0, 1, 2
 OBSTACLE_BOUNCE_BACK, OBSTACLE_PARTIAL = 0, 1
 STEP_MACRO = 1
 SERVE_BATCHED, SERVE_SEQUENTIAL = 0, 1
+ADMIT_SHORTEST_FIRST, ADMIT_FIFO = 0, 1
+LAYOUT_AUTO, LAYOUT_COMPACT, LAYOUT_DENSE = 0, 1, 2
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 STORAGE_BYTES = {STORE_F64: 8, STORE_F32S: 4, STORE_F16S: 2}
 
@@ -120,6 +122,9 @@ SIGNATURES = {
     "llb_batch_query": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_batch_set_stream_priority": [_H, ctypes.c_int32],
     "llb_batch_set_wait_limit": [_H, ctypes.c_int64],
+    "llb_batch_set_stop": [_H, ctypes.c_int32, ctypes.c_int64],
+    "llb_batch_set_layout": [_H, ctypes.c_int32],
+    "llb_batch_get_layout": [_H, ctypes.POINTER(ctypes.c_int32)],
     "llb_batch_event_record": [_H, ctypes.c_int32],
     "llb_batch_event_elapsed_ms": [_H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)],
     "llb_batch_info": [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
@@ -129,6 +134,7 @@ SIGNATURES = {
     "llb_server_create": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
                           ctypes.POINTER(_H)],
     "llb_server_destroy": [_H],
+    "llb_server_set_admission": [_H, ctypes.c_int64, ctypes.c_int32],
     "llb_server_submit": [_H, ctypes.POINTER(_Desc), _P, ctypes.c_int32, ctypes.c_int64,
                           ctypes.POINTER(ctypes.c_int64)],
     "llb_server_poll": [_H, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)],
@@ -503,6 +509,21 @@ class CudaBatch:
         gives up (-1: default); for tests of the timeout path."""
         _bcheck(lib().llb_batch_set_wait_limit(self._b, polls), self._b)
 
+    def set_layout(self, layout: int):
+        """LAYOUT_AUTO (compacted planes for obstacle-rich lattices),
+        LAYOUT_COMPACT (for every lattice that has them) or LAYOUT_DENSE."""
+        _bcheck(lib().llb_batch_set_layout(self._b, layout), self._b)
+
+    @property
+    def layout(self) -> int:
+        v = ctypes.c_int32()
+        _bcheck(lib().llb_batch_get_layout(self._b, ctypes.byref(v)), self._b)
+        return v.value
+
+    def set_stop(self, slot: int, stop_step: int):
+        """The lattice in `slot` stops before step index stop_step (-1: never)."""
+        _bcheck(lib().llb_batch_set_stop(self._b, slot, stop_step), self._b)
+
     def record(self, slot: int):
         _bcheck(lib().llb_batch_event_record(self._b, slot), self._b)
 
@@ -544,6 +565,13 @@ class CudaServer:
         _check(lib().llb_server_create(device, storage, mode, int(budget_bytes), max_chunk_steps, ctypes.byref(s)))
         self._s, self.storage, self.mode, self.device = s, storage, mode, device
         self._shape = {}
+
+    def set_admission(self, max_resident_nodes: int = 0, order: int = 0):
+        """Batched mode: at most max_resident_nodes lattice nodes resident (0:
+        default) and the admission order (ADMIT_SHORTEST_FIRST or ADMIT_FIFO)."""
+        rc = lib().llb_server_set_admission(self._s, int(max_resident_nodes), order)
+        if rc != 0:
+            raise LLBError(rc, "llb_server_set_admission")
 
     def close(self):
         if getattr(self, "_s", None):

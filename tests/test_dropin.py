@@ -190,3 +190,57 @@ def test_cuda_policy_matches_omp_policy_trt(tmp_path):
     assert len(files) == 8
     for f in files:
         assert filecmp.cmp(omp["dir"] / f, cud["dir"] / f, shallow=False), f
+
+
+READ_BINS = [os.path.join(BIN, f"read_lattice_{p}") for p in ("serial", "cuda")]
+needs_read = pytest.mark.skipif(not all(os.path.exists(b) for b in READ_BINS), reason="read_lattice not built")
+
+
+def read_structure(exe, path, out):
+    p = subprocess.run([exe, path, out], capture_output=True, text=True, timeout=900)
+    assert p.returncode == 0, p.stderr[-1000:]
+    secs = float([ln for ln in p.stderr.splitlines() if ln.startswith("read seconds")][-1].split()[-1])
+    return open(out).read(), secs
+
+
+@needs_read
+@pytest.mark.parametrize("geom", ["cavity129", "channel_discs", "odd_corners_solid", "porous"])
+def test_fast_reader_equals_reference_reader(tmp_path, geom):
+    """Lattice<CUDAPolicy>(path) reads the lattice file with the library's
+    O(R*C) classification; its node vectors (print_lattice_structure with
+    nodes) equal those of the reference's reader, Lattice<SerialPolicy>(path)."""
+    if geom == "cavity129":
+        types = H.cavity_types(129)
+    elif geom == "channel_discs":
+        types = H.channel_types(60, 140, discs=[(30, 40, 8), (12, 90, 5), (45, 100, 6)])
+    elif geom == "odd_corners_solid":
+        types = H.channel_types(37, 53, discs=[(18, 20, 4)])
+        types[1:-1, 0] = H.BOUNDARY
+        types[:, 0] = H.INLET
+        types[20, 30] = H.SOLID
+    else:
+        types = H.porous_types(120, 150, seed=7)
+    lat = str(tmp_path / "lattice.txt")
+    H.write_lattice_file(lat, types)
+    ref, _ = read_structure(READ_BINS[0], lat, str(tmp_path / "serial.txt"))
+    got, _ = read_structure(READ_BINS[1], lat, str(tmp_path / "cuda.txt"))
+    assert len(ref) > 0 and got == ref
+
+
+@needs_read
+def test_fast_reader_loads_a_4096_lattice_in_seconds(tmp_path):
+    """The 4096 x 4096 porous channel (about 5.2 million listed nodes): the
+    reference's reader classifies it in O(N^2) (std::find per obstacle
+    neighbour); the fast reader takes seconds."""
+    lat = str(tmp_path / "porous4096.txt")
+    types = H.porous_types(4096, 4096)
+    R, C = types.shape
+    counts = [int((types == c).sum()) for c in range(6)]
+    i, j = np.nonzero(types != H.FLUID)
+    with open(lat, "w") as f:
+        f.write("2\n%d %d\n%s\n" % (R, C, " ".join(str(c) for c in counts)))
+        np.savetxt(f, np.stack([i, j, types[i, j]], axis=1), fmt="%d")
+    text, secs = read_structure(READ_BINS[1], lat, str(tmp_path / "cuda.txt"))
+    assert secs < 30.0, secs
+    n_fluid = text.count("\n")  # one line per node and a few header lines
+    assert n_fluid > counts[0]

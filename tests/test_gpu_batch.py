@@ -231,3 +231,50 @@ def test_batch_barrier_timeout_reports_and_recovers():
         b.synchronize()
         for slot, prob in zip(slots, PROBLEMS):
             check_against_oracle(b.lattice(slot), prob, steps)
+
+
+def test_batch_stop_step_holds_a_lattice():
+    """A lattice given a stop step is left as it is by later batch steps (its
+    state is the oracle's at that step) while the others run on; the stop is
+    set mid-run and reached inside a graph-replayed stretch."""
+    import llalbm_cuda as L
+
+    with L.CudaBatch(storage=L.STORE_F64) as b:
+        slots = [add(b, prob, 400) for prob in PROBLEMS]
+        b.step(10)
+        b.set_stop(slots[1], 47)
+        b.set_stop(slots[3], 200)
+        b.step(150)
+        b.set_stop(slots[3], -1)   # lifted before it was reached: runs on
+        b.step(9)
+        b.synchronize()
+        want = {slots[1]: 47}
+        for slot, prob in zip(slots, PROBLEMS):
+            view = b.lattice(slot)
+            steps = want.get(slot, 170)
+            assert view.t == steps, (prob[0], view.t)
+            check_against_oracle(view, prob, steps)
+
+
+@pytest.mark.parametrize("layout", ["auto", "compact", "dense"])
+def test_batch_layouts_bit_exact_and_switchable(layout):
+    """Every lattice equals the oracle bit for bit whichever planes the batch
+    steps it on (compacted or dense), including after the layout of the
+    attached lattices changes in the middle of the run."""
+    import llalbm_cuda as L
+
+    first = {"auto": L.LAYOUT_AUTO, "compact": L.LAYOUT_COMPACT, "dense": L.LAYOUT_DENSE}[layout]
+    then = L.LAYOUT_DENSE if first != L.LAYOUT_DENSE else L.LAYOUT_COMPACT
+    steps = 150
+    with L.CudaBatch(storage=L.STORE_F64) as b:
+        b.set_layout(first)
+        slots = [add(b, prob, steps + 2) for prob in PROBLEMS]
+        assert b.layout == first
+        b.step(61)
+        b.set_layout(then)
+        b.step(steps - 62)
+        b.synchronize()
+        for slot, prob in zip(slots, PROBLEMS):
+            view = b.lattice(slot)
+            assert view.t == steps
+            check_against_oracle(view, prob, steps)

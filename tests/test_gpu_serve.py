@@ -221,3 +221,31 @@ def test_small_lane_is_not_held_to_the_large_lattices_step_rate():
     np.testing.assert_array_equal(ub, alone["cavity64_long"][1])
     np.testing.assert_array_equal(ra, plain_big[0])
     np.testing.assert_array_equal(ua, plain_big[1])
+
+
+@pytest.mark.parametrize("order", ["shortest_first", "fifo"])
+def test_admission_order_under_the_node_cap(order):
+    """With room for one lattice at a time (resident-node cap), requests that
+    queue behind a running one are admitted shortest work first (lattice
+    nodes x steps) -- or in arrival order with ADMIT_FIFO."""
+    import llalbm_cuda as L
+
+    base = REQS[3]
+    first, longer, shorter = base[:5] + (50000,), base[:5] + (3000,), base[:5] + (300,)
+    nodes = base[1].rows * base[1].cols
+    with L.CudaServer(storage=L.STORE_F32S, budget_bytes=1 << 30, max_chunk_steps=64) as s:
+        s.set_admission(nodes, L.ADMIT_SHORTEST_FIRST if order == "shortest_first" else L.ADMIT_FIFO)
+        a = submit(s, first)
+        while s.state(a) != L.REQ_RUNNING:
+            time.sleep(0.0005)
+        b = submit(s, longer)
+        c = submit(s, shorter)
+        assert s.state(b) == L.REQ_QUEUED and s.state(c) == L.REQ_QUEUED
+        for r in (a, b, c):
+            s.wait(r, 120)
+        ta, tb, tc = (s.result(r, fields=False)[2] for r in (a, b, c))
+    assert tb[1] >= ta[2] and tc[1] >= ta[2]   # one lattice resident at a time
+    if order == "shortest_first":
+        assert tc[1] < tb[1] and tb[1] >= tc[2]
+    else:
+        assert tb[1] < tc[1] and tc[1] >= tb[2]
