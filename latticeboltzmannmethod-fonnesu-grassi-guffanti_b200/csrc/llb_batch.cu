@@ -40,6 +40,7 @@ struct llb_batch {
     int2* d_items = nullptr;
     int items_cap = 0;
     int n_items = 0;
+    int n_dense = 0;                     // items[0, n_dense): dense tiles; the rest compacted slot blocks
     long long step = 0;                  // batch step counter
     long long* d_sbase = nullptr;
     unsigned* d_bar = nullptr;           // [count, generation]
@@ -139,7 +140,7 @@ int rebuild(llb_batch_handle b) {
     drop_graph(b);
     b->order.clear();
     std::vector<BatchLattice> dev;
-    std::vector<int2> items;
+    std::vector<int2> items, slot_items;
     for (int s = 0; s < static_cast<int>(b->slot.size()); ++s) {
         if (!b->slot[s]) continue;
         const int idx = static_cast<int>(dev.size());
@@ -155,8 +156,10 @@ int rebuild(llb_batch_handle b) {
             const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
             n = static_cast<int64_t>(d.nti) * ntj;
         }
-        for (int64_t t = 0; t < n; ++t) items.push_back(make_int2(idx, static_cast<int>(t)));
+        for (int64_t t = 0; t < n; ++t) (d.compact ? slot_items : items).push_back(make_int2(idx, static_cast<int>(t)));
     }
+    const int n_dense = static_cast<int>(items.size());
+    items.insert(items.end(), slot_items.begin(), slot_items.end());
     LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
     if (static_cast<int>(dev.size()) > b->desc_cap) {
         if (b->d_desc) cudaFree(b->d_desc);
@@ -176,6 +179,7 @@ int rebuild(llb_batch_handle b) {
                                      b->stream));
     LLB_BCUDA(b, cudaStreamSynchronize(b->stream));
     b->n_items = static_cast<int>(items.size());
+    b->n_dense = n_dense;
     b->dirty = false;
     return LLB_OK;
 }
@@ -185,6 +189,7 @@ BatchLaunch launch_desc(llb_batch_handle b, long long soff, int steps) {
     L.lats = b->d_desc;
     L.items = b->d_items;
     L.n_items = b->n_items;
+    L.n_dense = b->n_dense;
     L.sbase = b->d_sbase;
     L.soff = soff;
     L.steps = steps;

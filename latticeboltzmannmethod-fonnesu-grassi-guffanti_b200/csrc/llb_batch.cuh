@@ -82,7 +82,7 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     if (t >= Lp->t_end) return;  // block-uniform: the lattice has finished
     const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
     T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
-    const Geometry g = Lp->g;
+    const Geometry& g = Lp->g;  // read where used (L1), not copied into registers
     const int nti = Lp->nti;
     unsigned* const flags = Lp->flags;
     const int i = (tile % nti) * BX + threadIdx.x;
@@ -133,11 +133,37 @@ __device__ __forceinline__ void batch_slots(const BatchLattice* __restrict__ Lp,
     const long long slot = static_cast<long long>(item) * nthr + threadIdx.y * blockDim.x + threadIdx.x;
     // the descriptor's fields are read where they are used (L1-resident), not
     // copied into registers
-    const bool bad = compact_slot<M, -1>(Lp->g, Lp->cg, Lp->ot, Lp->c, fin, fout, t, slot);
+    const bool bad = compact_slot<M, -1>(Lp->g, Lp->cg, Lp->ot, Lp->c, fin, fout, [t] { return t; }, slot);
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(Lp->flags, 1u);
 }
 
-// One launch: `steps` batch steps starting at batch step (*sbase + soff).
+// Resident blocks per SM of the one-step batch kernels: the largest count
+// whose register budget (48 for the shifted forms, 64 for FP64) holds the
+// path without spills.
+template <class M>
+__host__ __device__ constexpr int batch_min_blocks() { return sizeof(typename M::T) == 8 ? 4 : 5; }
+
+// One batch step, one block per item: the dense tiles (items[0, n)) ...
+template <class M>
+__global__ void __launch_bounds__(BX* BY, batch_min_blocks<M>()) k_batch_tiles(const BatchLattice* __restrict__ lats,
+                                                       const int2* __restrict__ items, const long long* sbase,
+                                                       long long soff) {
+    const int2 it = items[blockIdx.x];
+    batch_tile<M>(lats + it.x, it.y, *sbase + soff);
+}
+
+// ... and the compacted slot blocks, in a launch of their own (each kernel
+// gets the registers its own path needs).
+template <class M>
+__global__ void __launch_bounds__(BX* BY, batch_min_blocks<M>()) k_batch_slots(const BatchLattice* __restrict__ lats,
+                                                       const int2* __restrict__ items, const long long* sbase,
+                                                       long long soff) {
+    const int2 it = items[blockIdx.x];
+    batch_slots<M>(lats + it.x, it.y, *sbase + soff);
+}
+
+// One cooperative launch: `steps` batch steps starting at batch step
+// (*sbase + soff) over every item, a grid barrier between steps.
 template <class M>
 __global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __restrict__ lats,
                                                        const int2* __restrict__ items, int n_items,

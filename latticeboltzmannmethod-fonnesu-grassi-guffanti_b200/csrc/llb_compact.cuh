@@ -109,10 +109,13 @@ __device__ __forceinline__ void pull_compact_general(const Geometry& g, const Co
 // One slot per thread: a variant that gave each thread 2 (FP32) or 4 (FP16)
 // slots with all their loads issued first ran slower on B200 in every form
 // (porous 4096^2: FP16 103.7k -> 77.7k, FP32 98.3k -> 93.1k MLUPS).
-template <class M, int COLL>
+// tstep: callable returning the step index, evaluated for open nodes only (a
+// step index read from device memory stays off every other lane's path and
+// out of its registers).
+template <class M, int COLL, class TStep>
 __device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo& cg, const OpenTable& ot,
                                              const Collision& c, const typename M::T* __restrict__ fin,
-                                             typename M::T* __restrict__ fout, long long tstep, long long t) {
+                                             typename M::T* __restrict__ fout, TStep tstep, long long t) {
     const bool in = t < cg.n_slots;
     unsigned info = 0, nb = 0;
     if (in) {
@@ -162,7 +165,7 @@ __device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo
         typename M::R rr, xr, yr;
         if (cls == CLS_OPEN) {
             double rho, ux, uy;
-            open_node<M>(ot, g.open_idx[nb], m, tstep, f, rho, ux, uy);
+            open_node<M>(ot, g.open_idx[nb], m, tstep(), f, rho, ux, uy);
             rr = M::from_f64(rho);
             xr = static_cast<typename M::R>(ux);
             yr = static_cast<typename M::R>(uy);
@@ -187,7 +190,7 @@ __global__ void __launch_bounds__(COMPACT_BLOCK, 5) k_step_compact(Geometry g, C
                                                                    Collision c, const typename M::T* __restrict__ fin,
                                                                    typename M::T* __restrict__ fout, StepSync ss) {
     const long long t = static_cast<long long>(blockIdx.x) * COMPACT_BLOCK + threadIdx.x;
-    const bool bad = compact_slot<M, COLL>(g, cg, ot, c, fin, fout, current_step(ss), t);
+    const bool bad = compact_slot<M, COLL>(g, cg, ot, c, fin, fout, [&] { return current_step(ss); }, t);
     flag_numerics(ss, bad);
 }
 

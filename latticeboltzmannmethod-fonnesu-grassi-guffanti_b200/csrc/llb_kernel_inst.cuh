@@ -174,8 +174,12 @@ cudaError_t do_batch_step(const BatchLaunch& b) {
     const dim3 block(BX, b.block_y);
     auto kern = k_batch_step<M>;
     if (!b.cooperative) {
-        kern<<<b.grid, block, 0, b.stream>>>(b.lats, b.items, b.n_items, b.sbase, b.soff, b.steps, b.bar, b.err,
-                                             b.bar_limit);
+        // one step: a block per item, dense tiles and compacted slot blocks in
+        // launches of their own
+        if (b.n_dense > 0) k_batch_tiles<M><<<b.n_dense, block, 0, b.stream>>>(b.lats, b.items, b.sbase, b.soff);
+        if (b.n_items > b.n_dense)
+            k_batch_slots<M><<<b.n_items - b.n_dense, block, 0, b.stream>>>(b.lats, b.items + b.n_dense, b.sbase,
+                                                                            b.soff);
         return cudaGetLastError();
     }
     const BatchLattice* lats = b.lats;

@@ -48,8 +48,9 @@ struct BatchLattice;
 // grid cooperatively (required when steps > 1).
 struct BatchLaunch {
     const BatchLattice* lats;
-    const int2* items;
+    const int2* items;     // dense tiles first, then compacted slot blocks
     int n_items;
+    int n_dense;          // items[0, n_dense) are dense tiles
     const long long* sbase;
     long long soff;
     int steps;

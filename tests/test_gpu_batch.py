@@ -153,10 +153,11 @@ def test_batch_f32s_matches_single_lattice():
             assert err <= 1e-6, (prob[0], err)
 
 
-def test_large_lattices_step_by_their_own_kernel_in_the_batch():
-    """Lattices of 2^20 nodes or more run their own default kernel inside the
-    batch step (the TMA pipeline for the porous channel, one thread per node
-    for the cavity), joining at different step parities and crossing graph
+def test_large_lattices_are_items_of_the_one_work_list():
+    """Lattices of 2^20 nodes or more are tiles or slot blocks of the same work
+    list as the small ones (one launch per batch step): the porous channel on
+    its compacted planes (its single-lattice default too), the cavity on the
+    dense ones, joining at different step parities and crossing graph
     replays and single steps; every lattice stays bit-exact."""
     import llalbm_cuda as L
 
@@ -166,7 +167,7 @@ def test_large_lattices_step_by_their_own_kernel_in_the_batch():
     big_cav = ("cavity1024", cav, H.Params.trt_magic(0.7), "const:0.05:0", "const:0:0")
     with L.CudaLattice(por.rows, por.cols, por.fluid, por.wall, por.inlet, por.inlet_side, por.outlet,
                        por.outlet_side, por.obstacle, por.obstacle_dirs) as g:
-        assert g.pipeline >= 0                      # TMA pipeline by default
+        assert g.pipeline == -3                     # compacted planes by default
     with L.CudaLattice(cav.rows, cav.cols, cav.fluid, cav.wall, cav.inlet, cav.inlet_side, cav.outlet,
                        cav.outlet_side, cav.obstacle, cav.obstacle_dirs) as g:
         assert g.pipeline == -1                     # one thread per node
