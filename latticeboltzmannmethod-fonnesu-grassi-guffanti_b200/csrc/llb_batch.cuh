@@ -137,11 +137,12 @@ __device__ __forceinline__ void batch_slots(const BatchLattice* __restrict__ Lp,
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(Lp->flags, 1u);
 }
 
-// Resident blocks per SM of the one-step batch kernels: the largest count
-// whose register budget (48 for the shifted forms, 64 for FP64) holds the
-// path without spills.
+// Resident blocks per SM of the one-step batch kernels (256-thread budget):
+// 6 for the shifted forms (40 registers, a few spilled: config 4 ran 64.2k
+// MLUPS against 61.7k at 5 blocks and 48 registers without spills), 4 for
+// FP64 (64 registers, no spills).
 template <class M>
-__host__ __device__ constexpr int batch_min_blocks() { return sizeof(typename M::T) == 8 ? 4 : 5; }
+__host__ __device__ constexpr int batch_min_blocks() { return sizeof(typename M::T) == 8 ? 4 : 6; }
 
 // One batch step, one block per item: the dense tiles (items[0, n)) ...
 template <class M>

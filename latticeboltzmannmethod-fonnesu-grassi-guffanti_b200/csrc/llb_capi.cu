@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -48,12 +49,46 @@ int cuda_fail(llb_handle h, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
     } while (0)
 
+// Device memory of lattices comes from a stream-ordered pool per device that
+// the library owns.  A lattice's buffers are allocated and freed in the order
+// of its stream (cudaMallocFromPoolAsync / cudaFreeAsync), so retiring a
+// lattice never synchronises the device -- cudaFree can, and a solve server
+// retiring lattices would stall every other lattice's kernels -- and the pool
+// keeps freed memory for the next lattice rather than returning it to the
+// driver at each synchronisation.
+constexpr int MAX_POOL_DEVICES = 64;
+cudaMemPool_t lattice_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[MAX_POOL_DEVICES] = {};
+    if (device < 0 || device >= MAX_POOL_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
 template <typename T>
 int dev_alloc(llb_handle h, T** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+    cudaMemPool_t pool = lattice_pool(h->device);
+    if (!pool) return fail(h, LLB_E_CUDA, "device memory pool unavailable");
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMallocFromPoolAsync");
     h->bytes += static_cast<int64_t>(bytes);
     return LLB_OK;
+}
+
+// Returns a buffer to the pool in the order of the handle's stream.
+void dev_free(llb_handle h, void* p) {
+    if (p) cudaFreeAsync(p, h->stream);
 }
 
 int select_device(llb_handle h) {
@@ -101,8 +136,7 @@ void release(llb_handle h) {
     void* bufs[] = {h->f[0], h->f[1], h->d_mask, h->d_bb, h->d_ps, h->d_psb, h->d_sectors, h->d_smask, h->d_sbb, h->d_open_idx, h->d_open, h->d_rho, h->d_u, h->d_dense,
                     h->d_step, h->d_flags, h->d_partials, h->d_red, h->d_fpts, h->d_fdirs, h->d_gather,
                     h->cf[0], h->cf[1], h->d_cnb, h->d_cseg, h->d_cchunk, h->d_ccol, h->d_cinfo};
-    for (void* b : bufs)
-        if (b) cudaFree(b);
+    for (void* b : bufs) dev_free(h, b);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
@@ -224,7 +258,7 @@ int build_mask(const llb_desc* d, int ld, std::vector<uint8_t>& mask, std::vecto
 
 int ensure_partials(llb_handle h, int nblocks) {
     if (h->partial_blocks >= nblocks) return LLB_OK;
-    if (h->d_partials) { cudaFree(h->d_partials); h->d_partials = nullptr; }
+    if (h->d_partials) { dev_free(h, h->d_partials); h->d_partials = nullptr; }
     int rc = dev_alloc(h, &h->d_partials, sizeof(double2) * 3 * static_cast<size_t>(nblocks));
     if (rc) return rc;
     h->partial_blocks = nblocks;
@@ -328,7 +362,7 @@ int state_to_compact(llb_handle h) {
 void release_compact(llb_handle h) {
     for (void* p : {h->cf[0], h->cf[1], static_cast<void*>(h->d_cnb), static_cast<void*>(h->d_cseg),
                     static_cast<void*>(h->d_cchunk), static_cast<void*>(h->d_ccol), static_cast<void*>(h->d_cinfo)})
-        if (p) cudaFree(p);
+        dev_free(h, p);
     h->cf[0] = h->cf[1] = nullptr;
     h->d_cnb = nullptr;
     h->d_cseg = nullptr;
@@ -450,7 +484,7 @@ int build_compact_from(llb_handle h, const std::vector<uint8_t>& mask, const std
     if (rc) {
         for (void* p : {cf0, cf1, static_cast<void*>(d_seg), static_cast<void*>(d_chunk), static_cast<void*>(d_col),
                         static_cast<void*>(d_info), static_cast<void*>(d_nb)})
-            if (p) cudaFree(p);
+            dev_free(h, p);
         h->bytes = before;
         return rc;
     }
@@ -912,7 +946,7 @@ int llb_set_force_points(llb_handle h, const int64_t* ij, const uint16_t* dirs, 
     if (rc) return rc;
     LLB_CUDA(h, cudaStreamSynchronize(h->stream));
     for (void* p : {static_cast<void*>(h->d_fpts), static_cast<void*>(h->d_fdirs), static_cast<void*>(h->d_gather)})
-        if (p) cudaFree(p);
+        dev_free(h, p);
     h->d_fpts = nullptr;
     h->d_fdirs = nullptr;
     h->d_gather = nullptr;
@@ -1064,7 +1098,7 @@ static int build_sector_list(llb_handle h) {
         void* bufs[3] = {d_sec, d_sm, d_sb};
         for (int q = 0; q < 3; ++q)
             if (bufs[q]) {
-                cudaFree(bufs[q]);
+                dev_free(h, bufs[q]);
                 h->bytes -= static_cast<int64_t>(sizes[q]);
             }
         return rc;
@@ -1109,9 +1143,9 @@ int llb_get_pipeline(llb_handle h, int32_t* config) {
 static void release_sector_list(llb_handle h) {
     const int64_t SN = LIST_BYTES / static_cast<int64_t>(h->elem);
     if (h->d_sectors) {
-        cudaFree(h->d_sectors);
-        cudaFree(h->d_smask);
-        cudaFree(h->d_sbb);
+        dev_free(h, h->d_sectors);
+        dev_free(h, h->d_smask);
+        dev_free(h, h->d_sbb);
         h->bytes -= static_cast<int64_t>(h->n_sectors) * (static_cast<int64_t>(sizeof(int32_t)) + 2 * SN);
     }
     h->d_sectors = nullptr;
