@@ -730,12 +730,12 @@ def serve_submit(server, p, steps=None):
                          outlet_bc=r["outlet_bc"], open_values=p["table"])
 
 
-def serve_stream(L, prepared, arrivals, storage, mode, budget, warmup):
+def serve_stream(L, prepared, arrivals, storage, mode, budget, warmup, max_chunk=1024):
     """Submits every request at its arrival time (a feeder thread), collects
     every result (rho and u copied to host memory); latency = done - submitted."""
     import queue as Q
 
-    with L.CudaServer(storage=storage, mode=mode, budget_bytes=budget, max_chunk_steps=256) as s:
+    with L.CudaServer(storage=storage, mode=mode, budget_bytes=budget, max_chunk_steps=max_chunk) as s:
         small = sorted(prepared, key=lambda p: p["req"]["rows"] * p["req"]["cols"])[:max(warmup, 1)]
         for p in small:                                   # warm-up: module load, first graphs
             rid = serve_submit(s, p, steps=200)
@@ -812,14 +812,15 @@ def run_serve(a, dist):
     resident = nodes * 128 / cap_ms / 1e3
     # capacity of the server: the whole stream submitted at once (the server is
     # never idle; admission, chunking, retirement and the tail included)
-    burst = serve_stream(L, prepared, np.zeros(len(prepared)), L.STORE_F32S, L.SERVE_BATCHED, budget, a.warmup)
+    burst = serve_stream(L, prepared, np.zeros(len(prepared)), L.STORE_F32S, L.SERVE_BATCHED, budget, a.warmup,
+                         a.max_chunk)
     cal = {"mlups": burst["mlups"]}
     capacity = cal["mlups"] * 1e6
     mean_work = np.mean([p["req"]["rows"] * p["req"]["cols"] * p["req"]["steps"] for p in prepared])
     rate = 0.7 * capacity / mean_work
     arrivals = W.poisson_arrivals(len(prepared), rate)
     sampler = ClockSampler(dist.local)
-    batched = serve_stream(L, prepared, arrivals, L.STORE_F32S, L.SERVE_BATCHED, budget, a.warmup)
+    batched = serve_stream(L, prepared, arrivals, L.STORE_F32S, L.SERVE_BATCHED, budget, a.warmup, a.max_chunk)
     clocks = sampler.summary(batched["t0"] - time.monotonic() + time.perf_counter(),
                              batched["t1"] - time.monotonic() + time.perf_counter())
     plain = serve_stream(L, prepared, arrivals, L.STORE_F64, L.SERVE_SEQUENTIAL, budget, a.warmup)
@@ -881,6 +882,8 @@ def main():
     ap.add_argument("--lattices", type=int, default=256,
                     help="batch256 workload: the first N of the 256 problems (smaller batches for profiling)")
     ap.add_argument("--requests", type=int, default=96, help="requests in the served stream (workload serve)")
+    ap.add_argument("--max-chunk", type=int, default=1024,
+                    help="served stream: steps per chunk of the batched server's lanes, at most")
     ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous and cavity workloads")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -264,7 +264,9 @@ int llb_batch_remove(llb_batch_handle b, int32_t slot);
 /* Moves a lattice made by llb_create (boundary values set; initialised or
    not -- step 0 then runs on the batch's stream) into the batch, so its
    creation and upload can happen elsewhere (another thread, another stream)
-   while the batch runs.  The batch owns it from then on. */
+   while the batch runs.  The batch owns it from then on.  A lattice whose
+   nine planes reach 2^31 slots (about 200 million nodes) is refused with
+   LLB_E_UNSUPPORTED: the batch's kernels use 32-bit slot offsets. */
 int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot);
 /* Takes a lattice out of the batch without destroying it: the caller owns
    the handle again (on a stream of its own that starts after the batch work

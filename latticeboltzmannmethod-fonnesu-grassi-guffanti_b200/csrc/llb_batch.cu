@@ -339,6 +339,9 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
         return bfail(b, LLB_E_INVALID, "lattice storage, pattern or device differs from the batch");
     if (!h->own_stream) return bfail(b, LLB_E_STATE, "lattice already belongs to a batch");
     if (h->d_ps) return bfail(b, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the single-lattice path");
+    // the batch's kernels index a lattice's nine planes with 32-bit offsets
+    if (10 * static_cast<int64_t>(h->plane) >= (int64_t{1} << 31))
+        return bfail(b, LLB_E_UNSUPPORTED, "lattice too large for a batch (its planes need 32-bit offsets)");
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
     // the batch steps the compacted planes (built here, on the lattice's own
     // stream, so a chunk running on the batch's stream is not waited for);

@@ -88,7 +88,10 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     const int i = (tile % nti) * BX + threadIdx.x;
     const int j = (tile / nti) * blockDim.y + threadIdx.y;
     const bool inside = i < g.rows && j < g.cols;
-    const long long node = static_cast<long long>(j) * g.ld + i;
+    // 32-bit slot arithmetic: a batch admits only lattices whose nine planes
+    // hold fewer than 2^31 slots
+    const int P = static_cast<int>(g.plane);
+    const int node = j * g.ld + i;
     const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
     const uint8_t cls = mask_class(m);
     const bool write_sector = sector_has_active<M>(class_active(cls));
@@ -96,7 +99,7 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     bool bad = false;
     if (inside && class_active(cls)) {
         typename M::R f[9];
-        pull<M>(g, fin, i, j, node, m, warp_plain, f);
+        pull<M, int>(g, fin, i, j, node, m, warp_plain, f);
         typename M::R rr, xr, yr;
         if (cls == CLS_OPEN) {
             double rho, ux, uy;
@@ -111,10 +114,10 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
         if (Lp->c.model == 0) M::template collide<0>(f, rr, xr, yr, Lp->c);
         else M::template collide<1>(f, rr, xr, yr, Lp->c);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, f[k]);
+        for (int k = 0; k < 9; ++k) M::store(fout + (k * P + node), f[k]);
     } else if (write_sector && j < g.cols && i < g.ld) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) M::store(fout + k * g.plane + node, M::keep(k));
+        for (int k = 0; k < 9; ++k) M::store(fout + (k * P + node), M::keep(k));
     }
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
 }
@@ -133,7 +136,8 @@ __device__ __forceinline__ void batch_slots(const BatchLattice* __restrict__ Lp,
     const long long slot = static_cast<long long>(item) * nthr + threadIdx.y * blockDim.x + threadIdx.x;
     // the descriptor's fields are read where they are used (L1-resident), not
     // copied into registers
-    const bool bad = compact_slot<M, -1>(Lp->g, Lp->cg, Lp->ot, Lp->c, fin, fout, [t] { return t; }, slot);
+    const bool bad =
+        compact_slot<M, -1, int>(Lp->g, Lp->cg, Lp->ot, Lp->c, fin, fout, [t] { return t; }, static_cast<int>(slot));
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(Lp->flags, 1u);
 }
 

@@ -112,10 +112,12 @@ __device__ __forceinline__ void pull_compact_general(const Geometry& g, const Co
 // tstep: callable returning the step index, evaluated for open nodes only (a
 // step index read from device memory stays off every other lane's path and
 // out of its registers).
-template <class M, int COLL, class TStep>
+// I: the type of the slot arithmetic (long long, or int where the nine planes
+// hold fewer than 2^31 slots).
+template <class M, int COLL, class I, class TStep>
 __device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo& cg, const OpenTable& ot,
                                              const Collision& c, const typename M::T* __restrict__ fin,
-                                             typename M::T* __restrict__ fout, TStep tstep, long long t) {
+                                             typename M::T* __restrict__ fout, TStep tstep, I t) {
     const bool in = t < cg.n_slots;
     unsigned info = 0, nb = 0;
     if (in) {
@@ -127,19 +129,19 @@ __device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo
     const bool node = class_active(cls);
     const bool general = cls == CLS_OPEN || (node && (m & COMPACT_DEAD_SRC));
     const bool warp_plain = __all_sync(0xffffffffu, !node || ((m & MASK_PLAIN) && !general));
-    const long long P = cg.cplane;
+    const I P = static_cast<I>(cg.cplane);
     bool bad = false;
     if (node) {
         typename M::R f[9];
         if (!general) {
             // fluid node: both neighbouring columns exist; a source that is not
             // a wall or obstacle is active
-            const long long cL = t - static_cast<long long>(nb & 0xffffu);
-            const long long cR = t + static_cast<long long>(nb >> 16);
+            const I cL = t - static_cast<I>(nb & 0xffffu);
+            const I cR = t + static_cast<I>(nb >> 16);
             const unsigned bb = (m & MASK_PLAIN) ? 0u : (info >> 8);
-            const long long aL = ((bb >> 0) & 1u) ? 0 : 1;  // row i of column j - 1 active (direction 1's source)
-            const long long aR = ((bb >> 2) & 1u) ? 0 : 1;  // row i of column j + 1 active (direction 3's source)
-            long long src[9];
+            const I aL = ((bb >> 0) & 1u) ? 0 : 1;  // row i of column j - 1 active (direction 1's source)
+            const I aR = ((bb >> 2) & 1u) ? 0 : 1;  // row i of column j + 1 active (direction 3's source)
+            I src[9];
             src[1] = cL;       // (i, j-1)
             src[2] = t + 1;    // (i+1, j)
             src[3] = cR;       // (i, j+1)
@@ -151,11 +153,11 @@ __device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo
             f[0] = M::load(fin + t);
             if (warp_plain) {
 #pragma unroll
-                for (int k = 1; k < 9; ++k) f[k] = M::load(fin + k * P + src[k]);
+                for (int k = 1; k < 9; ++k) f[k] = M::load(fin + (k * P + src[k]));
             } else {
 #pragma unroll
                 for (int k = 1; k < 9; ++k) {
-                    const long long a = ((bb >> (k - 1)) & 1u) ? opp(k) * P + t : k * P + src[k];
+                    const I a = ((bb >> (k - 1)) & 1u) ? opp(k) * P + t : k * P + src[k];
                     f[k] = M::load(fin + a);
                 }
             }
@@ -176,10 +178,10 @@ __device__ __forceinline__ bool compact_slot(const Geometry& g, const CompactGeo
         if (COLL == 0 || (COLL < 0 && c.model == 0)) M::template collide<0>(f, rr, xr, yr, c);
         else M::template collide<1>(f, rr, xr, yr, c);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) M::store(fout + k * P + t, f[k]);
+        for (int k = 0; k < 9; ++k) M::store(fout + (k * P + t), f[k]);
     } else if (in) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) M::store(fout + k * P + t, M::keep(k));
+        for (int k = 0; k < 9; ++k) M::store(fout + (k * P + t), M::keep(k));
     }
     return bad;
 }
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(COMPACT_BLOCK, 5) k_step_compact(Geometry g, C
                                                                    Collision c, const typename M::T* __restrict__ fin,
                                                                    typename M::T* __restrict__ fout, StepSync ss) {
     const long long t = static_cast<long long>(blockIdx.x) * COMPACT_BLOCK + threadIdx.x;
-    const bool bad = compact_slot<M, COLL>(g, cg, ot, c, fin, fout, [&] { return current_step(ss); }, t);
+    const bool bad = compact_slot<M, COLL, long long>(g, cg, ot, c, fin, fout, [&] { return current_step(ss); }, t);
     flag_numerics(ss, bad);
 }
 

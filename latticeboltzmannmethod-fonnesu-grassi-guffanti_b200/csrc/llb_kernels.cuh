@@ -31,22 +31,25 @@ constexpr int BX = 32, BY = MAX_BLOCK_Y;  // one warp = 32 rows of one column
 // path on every lane, where a bounce-back source is only another address
 // (plain lanes skip the bounce-bit load).
 // b_pre: the node's bounce byte when the caller has it already (NO_BB: load it).
+// I: the type of the slot arithmetic -- long long in general; int where every
+// offset of the nine planes fits in 32 bits (a batch's lattices), which saves
+// the 64-bit multiply-adds of the 18 accesses of a node.
 constexpr unsigned NO_BB = 0x100u;
-template <class M>
+template <class M, class I = long long>
 __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __restrict__ fin, int i, int j,
-                                     long long node, uint8_t m, bool warp_plain, typename M::R* f,
+                                     I node, uint8_t m, bool warp_plain, typename M::R* f,
                                      unsigned b_pre = NO_BB) {
+    const I P = static_cast<I>(g.plane), ld = static_cast<I>(g.ld);
     f[0] = M::load(fin + node);
     if (warp_plain) {
 #pragma unroll
-        for (int k = 1; k < 9; ++k) f[k] = M::load(fin + k * g.plane + node - (DJ(k) * g.ld + DI(k)));
+        for (int k = 1; k < 9; ++k) f[k] = M::load(fin + (k * P + node - (DJ(k) * ld + DI(k))));
     } else if (i > 0 && j > 0 && i < g.rows - 1 && j < g.cols - 1) {
         const unsigned b = (m & MASK_PLAIN) ? 0u : (b_pre != NO_BB ? b_pre : g.bb[node]);
 #pragma unroll
         for (int k = 1; k < 9; ++k) {
-            const typename M::T* p = ((b >> (k - 1)) & 1u) ? fin + opp(k) * g.plane + node
-                                                     : fin + k * g.plane + node - (DJ(k) * g.ld + DI(k));
-            f[k] = M::load(p);
+            const I a = ((b >> (k - 1)) & 1u) ? opp(k) * P + node : k * P + node - (DJ(k) * ld + DI(k));
+            f[k] = M::load(fin + a);
         }
     } else {
         // open nodes on the lattice edge: sources outside keep their initial value
@@ -55,11 +58,11 @@ __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __r
             const int si = i - DI(k), sj = j - DJ(k);
             typename M::R v = M::keep(k);
             if (si >= 0 && sj >= 0 && si < g.rows && sj < g.cols) {
-                const long long src = static_cast<long long>(sj) * g.ld + si;
+                const I src = static_cast<I>(sj) * ld + si;
                 // a bounce-back source reflects this node's own population; fluid,
                 // open and dead sources are read where they are
-                v = mask_class(g.mask[src]) == CLS_BB ? M::load(fin + opp(k) * g.plane + node)
-                                                      : M::load(fin + k * g.plane + src);
+                v = mask_class(g.mask[src]) == CLS_BB ? M::load(fin + (opp(k) * P + node))
+                                                      : M::load(fin + (k * P + src));
             }
             f[k] = v;
         }
