@@ -482,7 +482,8 @@ def run_ours(a, dist):
 
     # end to end through the C ABI with host buffers: every step copies its
     # boundary values from pinned host memory and reads back the step's
-    # stability flag (the reference's per-step LLALBM_DEBUG NaN scan).
+    # stability flag (the reference's per-step LLALBM_DEBUG NaN scan); the
+    # read-back of step n is awaited after step n + 1 is queued.
     try:
         import torch
         pinned = torch.empty((1, g.n_open, 2), dtype=torch.float64, pin_memory=True).numpy()
@@ -490,16 +491,20 @@ def run_ours(a, dist):
         pinned = np.empty((1, g.n_open, 2))
     pinned[...] = open_table(wl, nodes)
     e2e_steps = max(1, min(a.steps, 200))
-    for _ in range(3):
-        g.set_open_values(pinned, g.t)
-        g.step(1)
-        g.check_numerics()
+
+    def e2e_run(n):
+        for q in range(n):
+            g.set_open_values(pinned, g.t)
+            g.step(1)
+            g.check_numerics_begin(q % 2)
+            if q > 0:
+                g.check_numerics_end((q - 1) % 2)
+        g.check_numerics_end((n - 1) % 2)
+
+    e2e_run(3)
     dist.barrier()
     t_e = time.perf_counter()
-    for _ in range(e2e_steps):
-        g.set_open_values(pinned, g.t)
-        g.step(1)
-        g.check_numerics()
+    e2e_run(e2e_steps)
     e_s = dist.max(time.perf_counter() - t_e)
     g.close()
     sampler.stop()
@@ -534,7 +539,8 @@ def run_ours(a, dist):
                   for k, v in forms.items()},
         "e2e": {"value": round(dist.world * R * C * e2e_steps / e_s / 1e6, 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": int(pinned.nbytes), "d2h_bytes_per_step": 4, "steps": e2e_steps,
-                "path": "C ABI per step: llb_set_open_values (pinned host) + llb_step + llb_check_numerics"},
+                "path": "C ABI per step: llb_set_open_values (pinned host) + llb_step + llb_check_numerics_begin; "
+                        "the step's flag read back (llb_check_numerics_end) after the next step is queued"},
         "gpu_launches": a.steps,
         "clocks": clocks,
     }
@@ -730,7 +736,7 @@ def serve_submit(server, p, steps=None):
                          outlet_bc=r["outlet_bc"], open_values=p["table"])
 
 
-def serve_stream(L, prepared, arrivals, storage, mode, budget, warmup, max_chunk=1024):
+def serve_stream(L, prepared, arrivals, storage, mode, budget, warmup, max_chunk=256):
     """Submits every request at its arrival time (a feeder thread), collects
     every result (rho and u copied to host memory); latency = done - submitted."""
     import queue as Q
@@ -882,7 +888,7 @@ def main():
     ap.add_argument("--lattices", type=int, default=256,
                     help="batch256 workload: the first N of the 256 problems (smaller batches for profiling)")
     ap.add_argument("--requests", type=int, default=96, help="requests in the served stream (workload serve)")
-    ap.add_argument("--max-chunk", type=int, default=1024,
+    ap.add_argument("--max-chunk", type=int, default=256,
                     help="served stream: steps per chunk of the batched server's lanes, at most")
     ap.add_argument("--size", type=int, default=4096, help="lattice side of the porous and cavity workloads")
     ap.add_argument("--forms", default="f64,f32s,f16s", help="storage forms to time (f64 always first)")

@@ -265,8 +265,9 @@ int llb_batch_remove(llb_batch_handle b, int32_t slot);
    not -- step 0 then runs on the batch's stream) into the batch, so its
    creation and upload can happen elsewhere (another thread, another stream)
    while the batch runs.  The batch owns it from then on.  A lattice whose
-   nine planes reach 2^31 slots (about 200 million nodes) is refused with
-   LLB_E_UNSUPPORTED: the batch's kernels use 32-bit slot offsets. */
+   nine planes reach 2^31 slots (about 200 million nodes), or with 2^16
+   columns or more, is refused with LLB_E_UNSUPPORTED: the batch's kernels
+   use 32-bit slot offsets and 16-bit tile indices. */
 int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot);
 /* Takes a lattice out of the batch without destroying it: the caller owns
    the handle again (on a stream of its own that starts after the batch work
@@ -393,6 +394,14 @@ int llb_synchronize(llb_handle h);
    (the reference's LLALBM_DEBUG NaN scan, Lattice.hpp:412-422), LLB_E_TIMEOUT
    if a pipelined kernel gave up a bounded wait; clears the flags. */
 int llb_check_numerics(llb_handle h);
+/* The same check in two halves, so the host need not wait for the step it
+   just queued: _begin enqueues, on the handle's stream, a copy of the flag
+   word into pinned host memory (slot in [0, 8)) and its reset, and returns;
+   _end waits for that copy and returns what llb_check_numerics would have.
+   A caller queues step n + 1 before it ends the check of step n, and the GPU
+   never idles on the read-back.  No reference counterpart. */
+int llb_check_numerics_begin(llb_handle h, int32_t slot);
+int llb_check_numerics_end(llb_handle h, int32_t slot);
 /* CUDA events on the handle's stream: slot in [0, 8). */
 int llb_event_record(llb_handle h, int32_t slot);
 int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, float* ms);

@@ -149,14 +149,15 @@ int rebuild(llb_batch_handle b) {
         // every lattice, large or small, is items of the one work list: one
         // persistent launch advances the whole batch
         const BatchLattice& d = b->desc[s];
-        int64_t n;
         if (d.compact) {
-            n = (d.cg.n_slots + slots_per_item(b) - 1) / slots_per_item(b);
+            const int64_t n = (d.cg.n_slots + slots_per_item(b) - 1) / slots_per_item(b);
+            for (int64_t t = 0; t < n; ++t) slot_items.push_back(make_int2(idx, static_cast<int>(t)));
         } else {
+            // tiles in column-major order, (row tile, column tile) packed in 16 bits each
             const int ntj = (d.g.cols + b->block_y - 1) / b->block_y;
-            n = static_cast<int64_t>(d.nti) * ntj;
+            for (int tj = 0; tj < ntj; ++tj)
+                for (int ti = 0; ti < d.nti; ++ti) items.push_back(make_int2(idx, ti | (tj << 16)));
         }
-        for (int64_t t = 0; t < n; ++t) (d.compact ? slot_items : items).push_back(make_int2(idx, static_cast<int>(t)));
     }
     const int n_dense = static_cast<int>(items.size());
     items.insert(items.end(), slot_items.begin(), slot_items.end());
@@ -339,9 +340,11 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
         return bfail(b, LLB_E_INVALID, "lattice storage, pattern or device differs from the batch");
     if (!h->own_stream) return bfail(b, LLB_E_STATE, "lattice already belongs to a batch");
     if (h->d_ps) return bfail(b, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the single-lattice path");
-    // the batch's kernels index a lattice's nine planes with 32-bit offsets
-    if (10 * static_cast<int64_t>(h->plane) >= (int64_t{1} << 31))
-        return bfail(b, LLB_E_UNSUPPORTED, "lattice too large for a batch (its planes need 32-bit offsets)");
+    // the batch's kernels index a lattice's nine planes with 32-bit offsets,
+    // and a dense tile's row and column tile indices with 16 bits each
+    if (10 * static_cast<int64_t>(h->plane) >= (int64_t{1} << 31) || (h->R + BX - 1) / BX >= (1 << 16) ||
+        h->C >= (1 << 16))
+        return bfail(b, LLB_E_UNSUPPORTED, "lattice too large for a batch (32-bit plane offsets, 16-bit tile indices)");
     if (cudaSetDevice(b->device) != cudaSuccess) return LLB_E_CUDA;
     // the batch steps the compacted planes (built here, on the lattice's own
     // stream, so a chunk running on the batch's stream is not waited for);

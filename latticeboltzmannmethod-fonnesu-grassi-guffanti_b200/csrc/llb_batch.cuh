@@ -71,8 +71,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, uns
     return ok_sh != 0;
 }
 
-// One tile of one lattice.  The descriptor fields are read once into
-// registers (the stores below cannot alias them).
+// One tile of one lattice: `tile` packs its row-tile index (low 16 bits) and
+// column-tile index (high 16 bits), computed on the host.
 template <class M>
 __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, int tile, long long s) {
     using T = typename M::T;
@@ -83,10 +83,9 @@ __device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, 
     const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
     T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
     const Geometry& g = Lp->g;  // read where used (L1), not copied into registers
-    const int nti = Lp->nti;
     unsigned* const flags = Lp->flags;
-    const int i = (tile % nti) * BX + threadIdx.x;
-    const int j = (tile / nti) * blockDim.y + threadIdx.y;
+    const int i = (tile & 0xffff) * BX + threadIdx.x;
+    const int j = (static_cast<unsigned>(tile) >> 16) * blockDim.y + threadIdx.y;
     const bool inside = i < g.rows && j < g.cols;
     // 32-bit slot arithmetic: a batch admits only lattices whose nine planes
     // hold fewer than 2^31 slots

@@ -139,6 +139,9 @@ void release(llb_handle h) {
     for (void* b : bufs) dev_free(h, b);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : h->flag_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -1017,6 +1020,13 @@ int llb_synchronize(llb_handle h) {
     return LLB_OK;
 }
 
+// The flag word's meaning, shared by the whole and the split checks.
+static int numerics_status(llb_handle h, unsigned flags) {
+    if (flags & 2u) return fail(h, LLB_E_TIMEOUT, "a pipelined step kernel gave up waiting for its copies");
+    if (flags & 1u) return fail(h, LLB_E_NUMERIC, "non-finite density detected");
+    return LLB_OK;
+}
+
 int llb_check_numerics(llb_handle h) {
     if (!h) return fail(nullptr, LLB_E_INVALID, "null handle");
     int rc = select_device(h);
@@ -1025,9 +1035,28 @@ int llb_check_numerics(llb_handle h) {
     LLB_CUDA(h, cudaMemcpyAsync(&flags, h->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
     LLB_CUDA(h, cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream));
     LLB_CUDA(h, cudaStreamSynchronize(h->stream));
-    if (flags & 2u) return fail(h, LLB_E_TIMEOUT, "a pipelined step kernel gave up waiting for its copies");
-    if (flags & 1u) return fail(h, LLB_E_NUMERIC, "non-finite density detected");
+    return numerics_status(h, flags);
+}
+
+int llb_check_numerics_begin(llb_handle h, int32_t slot) {
+    if (!h || slot < 0 || slot >= 8) return fail(h, LLB_E_INVALID, "bad arguments");
+    int rc = select_device(h);
+    if (rc) return rc;
+    if (!h->h_flags) LLB_CUDA(h, cudaHostAlloc(reinterpret_cast<void**>(&h->h_flags), 8 * sizeof(unsigned), cudaHostAllocDefault));
+    if (!h->flag_ev[slot]) LLB_CUDA(h, cudaEventCreateWithFlags(&h->flag_ev[slot], cudaEventDisableTiming));
+    LLB_CUDA(h, cudaMemcpyAsync(&h->h_flags[slot], h->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    LLB_CUDA(h, cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream));
+    LLB_CUDA(h, cudaEventRecord(h->flag_ev[slot], h->stream));
     return LLB_OK;
+}
+
+int llb_check_numerics_end(llb_handle h, int32_t slot) {
+    if (!h || slot < 0 || slot >= 8) return fail(h, LLB_E_INVALID, "bad arguments");
+    if (!h->flag_ev[slot]) return fail(h, LLB_E_STATE, "no llb_check_numerics_begin on this slot");
+    int rc = select_device(h);
+    if (rc) return rc;
+    LLB_CUDA(h, cudaEventSynchronize(h->flag_ev[slot]));
+    return numerics_status(h, h->h_flags[slot]);
 }
 
 int llb_event_record(llb_handle h, int32_t slot) {

@@ -55,6 +55,10 @@ struct llb_lattice {
     bool initialized = false;
     bool macro_valid = false;
     cudaEvent_t ev[8] = {};
+    // split numerics checks: pinned host copies of the flag word and the
+    // events that mark their arrival, one per slot (allocated on first use)
+    unsigned* h_flags = nullptr;
+    cudaEvent_t flag_ev[8] = {};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t bytes = 0;
     std::string err;

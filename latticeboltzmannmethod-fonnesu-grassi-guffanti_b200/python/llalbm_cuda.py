@@ -104,6 +104,8 @@ SIGNATURES = {
     "llb_tune_pipeline": [_H, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
     "llb_set_launch_shape": [_H, ctypes.c_int32],
     "llb_set_wait_limit": [_H, ctypes.c_int64],
+    "llb_check_numerics_begin": [_H, ctypes.c_int32],
+    "llb_check_numerics_end": [_H, ctypes.c_int32],
     "llb_compute_macro": [_H, _P, _P],
     "llb_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_H)],
     "llb_batch_destroy": [_H],
@@ -309,6 +311,14 @@ class CudaLattice:
 
     def check_numerics(self):
         _check(lib().llb_check_numerics(self._h), self._h)
+
+    def check_numerics_begin(self, slot: int = 0):
+        """Queues the numerics check of the steps so far (slot in [0, 8))."""
+        _check(lib().llb_check_numerics_begin(self._h, slot), self._h)
+
+    def check_numerics_end(self, slot: int = 0):
+        """Waits for the check queued on `slot`; raises as check_numerics."""
+        _check(lib().llb_check_numerics_end(self._h, slot), self._h)
 
     # -- results -----------------------------------------------------------------
     def macro(self):

@@ -388,3 +388,29 @@ def test_pipelined_wait_timeout_reports_and_recovers(pipeline):
     act = H.active_mask(lists)
     np.testing.assert_array_equal(pop[:, act], ref["populations"][:, act])
     np.testing.assert_array_equal(u, ref["u"])
+
+
+def test_split_numerics_check():
+    """llb_check_numerics_begin/_end report what llb_check_numerics reports,
+    per slot, while later steps are already queued."""
+    import llalbm_cuda as L
+
+    lists = H.classify(H.cavity_types(32))
+    with make_gpu(lists, H.Params(tau=0.7)) as g:
+        g.set_open_values(H.open_values(lists, "const:0.05:0", "const:0:0", 1))
+        g.init()
+        for q in range(6):
+            g.step(1)
+            g.check_numerics_begin(q % 2)
+            if q:
+                g.check_numerics_end((q - 1) % 2)
+        g.check_numerics_end(1)
+    with make_gpu(lists, H.Params(tau=0.5001)) as g:
+        g.set_open_values(H.open_values(lists, "const:0.6:0", "const:0:0", 1))
+        g.init()
+        g.step(5000)
+        g.check_numerics_begin(3)
+        g.step(10)
+        with pytest.raises(L.LLBError) as e:
+            g.check_numerics_end(3)
+        assert e.value.code == -7
