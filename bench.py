@@ -656,7 +656,12 @@ def run_batch(a, dist):
     for p in probs:
         _, act = batch_add(b, L, p, L.STORE_F32S)
         active += act
-    by, spl, tune_ms = b.tune(8)
+    if a.batch_layout is None:
+        by, spl, tune_ms = b.tune(8)
+    else:  # a fixed layout and launch shape (profiling), no tuner
+        b.set_layout({"auto": 0, "compact": 1, "dense": 2}[a.batch_layout])
+        by, spl, tune_ms = a.batch_block_y, a.batch_spl, 0.0
+        b.set_config(by, spl)
     layout = {0: "auto", 1: "compact", 2: "dense"}[b.layout]
     b.step(a.warmup)
     b.synchronize()
@@ -887,6 +892,10 @@ def main():
     ap.add_argument("--launch-shape", type=int, default=None, help="columns per block of the one-thread kernel")
     ap.add_argument("--lattices", type=int, default=256,
                     help="batch256 workload: the first N of the 256 problems (smaller batches for profiling)")
+    ap.add_argument("--batch-layout", choices=("auto", "compact", "dense"), default=None,
+                    help="batch workload: fixed layout (with --batch-block-y / --batch-spl) instead of the autotuner")
+    ap.add_argument("--batch-block-y", type=int, default=2)
+    ap.add_argument("--batch-spl", type=int, default=1)
     ap.add_argument("--requests", type=int, default=96, help="requests in the served stream (workload serve)")
     ap.add_argument("--max-chunk", type=int, default=256,
                     help="served stream: steps per chunk of the batched server's lanes, at most")
