@@ -427,7 +427,11 @@ int llb_server_create(int32_t device, int32_t storage, int32_t mode, int64_t bud
         for (auto& b : s->batch) {
             const int rc = llb_batch_create(device, storage, &b);
             if (rc != LLB_OK) return drop(rc);
-            llb_batch_set_config(b, 8, 1);
+            // the batch autotuner's choice on mixed request streams (config 4
+            // and 5 alike): compacted planes, 32 x 2 threads per block, one
+            // step per launch
+            llb_batch_set_layout(b, LLB_LAYOUT_COMPACT);
+            llb_batch_set_config(b, 2, 1);
         }
         // the small lane's blocks go first, so small requests keep their own
         // step rate beside large lattices
