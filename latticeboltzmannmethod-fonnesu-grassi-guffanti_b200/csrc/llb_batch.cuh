@@ -141,11 +141,12 @@ __device__ __forceinline__ void batch_slots(const BatchLattice* __restrict__ Lp,
 }
 
 // Resident blocks per SM of the one-step batch kernels (256-thread budget):
-// 6 for the shifted forms (40 registers, a few spilled: config 4 ran 64.2k
-// MLUPS against 61.7k at 5 blocks and 48 registers without spills), 4 for
-// FP64 (64 registers, no spills).
+// 8 for the shifted forms (32 registers, full occupancy, some words spilled:
+// the 256 problems of config 4 ran 67.9k MLUPS against 64.7k at 6 blocks and
+// 40 registers, and 61.7k at 5 blocks and 48 registers), 4 for FP64 (64
+// registers, no spills).
 template <class M>
-__host__ __device__ constexpr int batch_min_blocks() { return sizeof(typename M::T) == 8 ? 4 : 6; }
+__host__ __device__ constexpr int batch_min_blocks() { return sizeof(typename M::T) == 8 ? 4 : 8; }
 
 // One batch step, one block per item: the dense tiles (items[0, n)) ...
 template <class M>

@@ -58,8 +58,16 @@ cudaError_t do_step_compact(const LaunchCtx& x, const CompactGeo& cg, const void
     const unsigned blocks = static_cast<unsigned>((cg.n_slots + COMPACT_BLOCK - 1) / COMPACT_BLOCK);
     const T* in = static_cast<const T*>(fin);
     T* out = static_cast<T*>(fout);
-    if (x.c.model == 0) k_step_compact<M, 0><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, x.ot, x.c, in, out, x.ss);
-    else k_step_compact<M, 1><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, x.ot, x.c, in, out, x.ss);
+#define LLB_COMPACT(COLL, I) \
+    k_step_compact<M, COLL, I><<<blocks, COMPACT_BLOCK, 0, x.stream>>>(x.g, cg, x.ot, x.c, in, out, x.ss)
+    if (cg.cplane * 9 < (1LL << 31)) {
+        if (x.c.model == 0) LLB_COMPACT(0, int);
+        else LLB_COMPACT(1, int);
+    } else {
+        if (x.c.model == 0) LLB_COMPACT(0, long long);
+        else LLB_COMPACT(1, long long);
+    }
+#undef LLB_COMPACT
     return cudaGetLastError();
 }
 
