@@ -10,6 +10,23 @@
 
 namespace llb {
 
+// Launch of kernel k with programmatic stream serialization (the kernel waits
+// for the previous one itself: pdl_wait_then_release).
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <class M>
 cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, bool macro) {
     using T = typename M::T;
@@ -17,9 +34,12 @@ cudaError_t do_step(const LaunchCtx& x, const void* fin, void* fout, bool init, 
     const dim3 block(BX, by), grid = node_grid(x.g, BX, by);
     const T* in = static_cast<const T*>(fin);
     T* out = static_cast<T*>(fout);
-#define LLB_STEP(COLL, MAC, INI) k_step<M, COLL, MAC, INI><<<grid, block, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss)
+    // the one-thread-per-node steps overlap their launch with the previous
+    // step's drain (small lattices are launch-bound)
+#define LLB_STEP(COLL, MAC, INI) \
+    return launch_pdl(k_step<M, COLL, MAC, INI>, grid, block, x.stream, x.g, x.ot, x.c, in, out, x.mo, x.ss)
 #define LLB_STEP_PS(COLL, MAC, INI) \
-    k_step<M, COLL, MAC, INI, true><<<grid, block, 0, x.stream>>>(x.g, x.ot, x.c, in, out, x.mo, x.ss)
+    return launch_pdl(k_step<M, COLL, MAC, INI, true>, grid, block, x.stream, x.g, x.ot, x.c, in, out, x.mo, x.ss)
     if constexpr (std::is_same_v<M, ModelF64>) {
         if (x.g.ps) {  // partially saturated obstacles
             if (x.c.model == 0) {

@@ -246,6 +246,18 @@ __device__ __forceinline__ void step_node(const Geometry& g, const OpenTable& ot
     flag_numerics(ss, bad);
 }
 
+// Programmatic dependent launch: a step kernel launched with programmatic
+// stream serialization may start while the previous kernel on the stream
+// drains.  It reads the lattice's own tables first (they do not change
+// between steps), then waits (griddepcontrol.wait returns once the previous
+// grid has completed and its writes are visible) before it touches the
+// populations, and lets the next step's launch begin as soon as every block
+// is past that point.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait_then_release() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // Block: 32 rows (one warp per column) x blockDim.y columns, blockDim.y <= BY.
 template <class M, int COLL, bool MACRO, bool INIT, bool PS = false>
 __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Collision c,
@@ -257,6 +269,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
     const long long node = static_cast<long long>(j) * g.ld + i;
     const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
     const bool write_sector = sector_has_active<M>(class_active(mask_class(m)));
+    pdl_wait_then_release();
     step_node<M, COLL, MACRO, INIT, PS>(g, ot, c, fin, fout, mo, ss, i, j, node, inside, m, write_sector,
                                         j < g.cols && i < g.ld);
 }
