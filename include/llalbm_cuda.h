@@ -411,16 +411,26 @@ int llb_event_elapsed_ms(llb_handle h, int32_t slot_begin, int32_t slot_end, flo
    two-steps-per-pass kernel (3..5: the intermediate step stays in shared
    memory, so a pair of steps reads and writes the populations once; a lone
    step runs on the one-thread kernel), the one-thread-per-node kernel for
-   config -1, or for config -2 one thread per node of every 32-byte population
-   sector that holds an active node (a list built on first use; lattices with
-   partially saturated obstacles or 2^31 or more slots per plane have none).
-   All compute the same per-node arithmetic: FP64 results are identical; the
-   shifted forms may differ in the last bits, as their kernels may contract
-   multiply-adds differently. */
+   config -1, for config -2 one thread per node of every 32-byte population
+   sector that holds an active node (a list built on first use), for config -3
+   one thread per slot of compacted planes that store only the fluid and open
+   nodes (built on first use; the default for obstacle-rich lattices of 2^18
+   nodes or more), and for config -4 the lattice resident in the shared memory
+   of one thread-block cluster of 16 blocks, up to 4096 steps per launch with
+   a cluster barrier between steps (lattices whose column slabs fit: about
+   129 x 129 in FP64, 181 x 181 in FP32, 256 x 256 in FP16; the default up to
+   12 000 nodes, 26 000 in FP16).  Lattices with partially saturated
+   obstacles run on config -1 only; lattices beyond the 32-bit limits of the
+   sector list or the compacted tables (2^31 slots; neighbouring columns more
+   than 65 535 slots apart) have no config -2 or -3, and lattices that do not
+   fit a cluster have no config -4 (LLB_E_UNSUPPORTED).  A lattice in a batch
+   (llb_batch_add) refuses -3: the batch's kernels step it.  All
+   configurations compute the same per-node arithmetic and give the same bits
+   in every storage form. */
 int llb_set_pipeline(llb_handle h, int32_t config);
 int llb_get_pipeline(llb_handle h, int32_t* config);
 /* Autotuner of one lattice (no reference counterpart): runs every plain-step
-   configuration this lattice supports (-1, -2, 0..6) for trial_steps warm-up
+   configuration this lattice supports (-4..-1, 0..6) for trial_steps warm-up
    and trial_steps timed steps and keeps the fastest.  Every configuration
    gives the same bits, so these are ordinary steps of the simulation: the
    lattice advances by 2 x trial_steps per configuration tried (llb_get_step

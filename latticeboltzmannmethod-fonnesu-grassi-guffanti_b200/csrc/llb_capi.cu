@@ -517,6 +517,16 @@ int build_compact(llb_handle h) {
     return build_compact_from(h, mask, bb);
 }
 
+// Whether the lattice fits one thread-block cluster (looked up once).
+bool cluster_ok(llb_handle h) {
+    if (h->cl_state == 0)
+        h->cl_state = (!h->d_ps && cluster_plan(h->storage, static_cast<int>(h->R), static_cast<int>(h->C), h->device,
+                                                &h->cl_plan))
+                          ? 1
+                          : -1;
+    return h->cl_state > 0;
+}
+
 // One step kernel (two steps for a two-step configuration unless `single`).
 // Inside a graph capture the step index is relative (graph_offset >= 0, base
 // read from d_step); otherwise it is absolute.
@@ -594,6 +604,14 @@ int batch_max_grid(int s, int block_y, int sm_count) {
 }
 cudaError_t launch_macro_now(int s, const LaunchCtx& x, const void* fin, long long t, double* rho, double* u) {
     return s == LLB_STORE_F64 ? launch_macro_now_f64(x, fin, t, rho, u) : launch_macro_now_lowp(s, x, fin, t, rho, u);
+}
+bool cluster_plan(int s, int R, int C, int device, ClusterPlan* plan) {
+    return s == LLB_STORE_F64 ? cluster_plan_f64(R, C, device, plan) : cluster_plan_lowp(s, R, C, device, plan);
+}
+cudaError_t launch_step_cluster(int s, const LaunchCtx& x, const ClusterPlan& p, void* f0, void* f1, int cur,
+                                long long t0, int steps) {
+    return s == LLB_STORE_F64 ? launch_step_cluster_f64(x, p, f0, f1, cur, t0, steps)
+                              : launch_step_cluster_lowp(s, x, p, f0, f1, cur, t0, steps);
 }
 cudaError_t launch_step_compact(int s, const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
     return s == LLB_STORE_F64 ? launch_step_compact_f64(x, cg, fin, fout) : launch_step_compact_lowp(s, x, cg, fin, fout);
@@ -767,6 +785,8 @@ int llb_create(const llb_desc* d, llb_handle* out) {
 
     auto bail = [&](int code) { std::string m = h->err; release(h); return fail(nullptr, code, m); };
     if ((rc = select_device(h))) return bail(rc);
+    if (h->tma_cfg == PIPE_GRID && ps.empty() && cluster_default_size(*h) && cluster_ok(h))
+        h->tma_cfg = PIPE_CLUSTER;
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaStreamCreate"));
     e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
@@ -861,7 +881,7 @@ int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
     const bool compact = h->tma_cfg == PIPE_COMPACT;
     if (plain > 0 && (rc = compact ? state_to_compact(h) : state_to_dense(h))) return rc;
     if (plain > 0) h->where = compact ? RES_COMPACT : RES_DENSE;  // where the steps below leave it
-    if (plain >= GRAPH_STEPS) {
+    if (plain >= GRAPH_STEPS && h->tma_cfg != PIPE_CLUSTER) {
         cudaGraphExec_t g = nullptr;
         if ((rc = graph_for(h, &g))) return rc;
         while (plain >= GRAPH_STEPS) {
@@ -870,6 +890,18 @@ int llb_step(llb_handle h, int32_t nsteps, uint32_t flags) {
             LLB_CUDA(h, cudaGraphLaunch(g, h->stream));
             h->step += GRAPH_STEPS;
             plain -= GRAPH_STEPS;
+        }
+    }
+    if (h->tma_cfg == PIPE_CLUSTER) {
+        // chunks of steps, each one launch of the cluster
+        while (plain > 0) {
+            const int n = std::min<int32_t>(plain, CLUSTER_CHUNK);
+            cudaError_t e =
+                launch_step_cluster(h->storage, make_ctx(h), h->cl_plan, h->f[0], h->f[1], h->cur, h->step, n);
+            if (e != cudaSuccess) return cuda_fail(h, e, "cluster step kernel launch");
+            h->cur ^= n & 1;
+            h->step += n;
+            plain -= n;
         }
     }
     const int per = steps_per_launch(h);
@@ -1140,12 +1172,18 @@ static int build_sector_list(llb_handle h) {
 }
 
 int llb_set_pipeline(llb_handle h, int32_t config) {
-    if (!h || config < PIPE_COMPACT || config >= TMA_CONFIGS)
-        return fail(h, LLB_E_INVALID, "config must be -3, -2, -1 or in [0, 7)");
+    if (!h || config < PIPE_CLUSTER || config >= TMA_CONFIGS)
+        return fail(h, LLB_E_INVALID, "config must be -4, -3, -2, -1 or in [0, 7)");
     if (config != PIPE_GRID && h->d_ps)
         return fail(h, LLB_E_UNSUPPORTED, "partially saturated obstacles run on the one-thread-per-node kernel");
     if (config == PIPE_COMPACT && !h->own_stream)
         return fail(h, LLB_E_STATE, "a lattice in a batch is stepped by the batch's kernels");
+    if (config == PIPE_CLUSTER) {
+        int rc = select_device(h);
+        if (rc) return rc;
+        if (!cluster_ok(h))
+            return fail(h, LLB_E_UNSUPPORTED, "the lattice's column slabs do not fit the shared memory of one cluster");
+    }
     if (config != h->tma_cfg) {
         int rc = select_device(h);
         if (rc) return rc;
@@ -1198,7 +1236,7 @@ int llb_tune_pipeline(llb_handle h, int32_t trial_steps, int32_t* best, float* m
     const int original = h->tma_cfg;
     int chosen = original;
     float chosen_ms = -1.0f;
-    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, PIPE_COMPACT, 0, 1, 2, 3, 4, 5, 6};
+    static constexpr int kCandidates[] = {PIPE_GRID, PIPE_LIST, PIPE_COMPACT, PIPE_CLUSTER, 0, 1, 2, 3, 4, 5, 6};
     for (int cfg : kCandidates) {
         if (llb_set_pipeline(h, cfg) != LLB_OK) continue;  // not available for this lattice
         // warm-up (tensor maps, graphs), then the timed steps

@@ -12,6 +12,11 @@ cudaError_t launch_fill_keep_f64(const LaunchCtx& x, void* buf) { return do_fill
 cudaError_t launch_step_compact_f64(const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
     return do_step_compact<ModelF64>(x, cg, fin, fout);
 }
+bool cluster_plan_f64(int R, int C, int device, ClusterPlan* plan) { return do_cluster_plan<ModelF64>(R, C, device, plan); }
+cudaError_t launch_step_cluster_f64(const LaunchCtx& x, const ClusterPlan& p, void* f0, void* f1, int cur, long long t0,
+                                    int steps) {
+    return do_step_cluster<ModelF64>(x, p, f0, f1, cur, t0, steps);
+}
 cudaError_t launch_compact_copy_f64(const LaunchCtx& x, const CompactGeo& cg, void* dense, void* comp, bool to_compact) {
     return do_compact_copy<ModelF64>(x, cg, dense, comp, to_compact);
 }

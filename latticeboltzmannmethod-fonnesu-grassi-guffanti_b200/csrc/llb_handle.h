@@ -63,7 +63,8 @@ struct llb_lattice {
     int64_t bytes = 0;
     std::string err;
     // plain-step kernel: tma_cfg >= 0 the TMA pipeline configuration,
-    // PIPE_GRID the one-thread-per-node grid, PIPE_LIST the active-sector list
+    // PIPE_GRID the one-thread-per-node grid, PIPE_LIST the active-sector list,
+    // PIPE_COMPACT the compacted planes, PIPE_CLUSTER one cluster
     int tma_cfg = 0;
     TmaPlan plan;
     bool maps_ready = false;
@@ -88,6 +89,11 @@ struct llb_lattice {
     int where = 0;
     // polls of the pipelined kernels' stage waits before they give up
     long long wait_limit = llb::DEFAULT_WAIT_LIMIT;
+    // the lattice resident in one thread-block cluster (pipeline
+    // PIPE_CLUSTER): its plan, looked up once (cl_state 0 not yet, 1 it
+    // fits, -1 it does not)
+    llb::ClusterPlan cl_plan;
+    int cl_state = 0;
 };
 
 // Residence of the state (llb_lattice::where).  Steps of the compacted
@@ -108,8 +114,17 @@ constexpr int RES_DENSE = 0, RES_COMPACT = 1, RES_BOTH = 2;
 //    3, from 2^28 bytes), the TMA pipeline for FP16 (from 2^27 bytes); else
 //    one thread per node, which runs close to the copy bandwidth on open flow
 //    (there every node is active and the compacted planes only add their
-//    6 bytes of addressing per node).
-constexpr int PIPE_GRID = -1, PIPE_LIST = -2, PIPE_COMPACT = -3;
+//    6 bytes of addressing per node);
+//  * lattices resident in one 16-block cluster (their slabs fit its shared
+//    memory) up to 12 000 nodes (FP64, FP32) or 26 000 (FP16): the cluster
+//    runs a chunk of steps per launch (chosen at creation, where the device
+//    is known).  96^2 steps in 2.2 us against 3.0 us on the one-thread grid;
+//    at config 1 (129^2) the 16 SMs of one cluster are bound by the FP64
+//    arithmetic of 16 641 nodes (3.6 us against 3.1 us), so the grid keeps it.
+constexpr int PIPE_GRID = -1, PIPE_LIST = -2, PIPE_COMPACT = -3, PIPE_CLUSTER = -4;
+inline bool cluster_default_size(const llb_lattice& h) {
+    return h.R * h.C <= (h.storage == LLB_STORE_F16S ? 26000 : 12000);
+}
 constexpr int64_t TMA_MIN_NODES = 1 << 19;
 constexpr double TMA_MIN_NONPLAIN = 0.05;
 constexpr int64_t COMPACT_MIN_NODES = 1 << 18;

@@ -7,6 +7,7 @@
 #include "llb_pair.cuh"
 #include "llb_batch.cuh"
 #include "llb_compact.cuh"
+#include "llb_cluster.cuh"
 
 namespace llb {
 
@@ -89,6 +90,89 @@ cudaError_t do_step_compact(const LaunchCtx& x, const CompactGeo& cg, const void
     }
 #undef LLB_COMPACT
     return cudaGetLastError();
+}
+
+// Cluster plan of a lattice (llb_cluster.cuh): 16 blocks (8 where a
+// non-portable cluster of 16 cannot be placed), slabs of at most wmax
+// columns, the shared memory a block needs.  False when the slab and its
+// halos do not fit one block's shared memory or no cluster can be placed.
+template <class M>
+bool do_cluster_plan(int R, int C, int device, ClusterPlan* plan) {
+    using T = typename M::T;
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    if (R >= (1 << 16)) return false;  // the active-node list packs rows in 16 bits
+    for (int nc : {CLUSTER_MAX_CTAS, 8}) {
+        if (C < nc) continue;
+        const int wmax = (C + nc - 1) / nc;
+        const long long bytes = ClusterSmem{R, wmax + 2}.bytes<T>();
+        if (bytes > optin) continue;
+        bool ok = true;
+        for (auto k : {k_step_cluster<M, 0>, k_step_cluster<M, 1>}) {
+            // the most the device allows next to the kernel's static shared
+            // memory, so launches of every lattice's plan are valid
+            cudaFuncAttributes fa{};
+            if (cudaFuncGetAttributes(&fa, k) != cudaSuccess ||
+                bytes + static_cast<long long>(fa.sharedSizeBytes) > optin ||
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     optin - static_cast<int>(fa.sharedSizeBytes)) != cudaSuccess ||
+                (nc > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
+                ok = false;
+                break;
+            }
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(nc);
+            cfg.blockDim = dim3(BX, CLUSTER_THREADS / BX);
+            cfg.dynamicSmemBytes = static_cast<size_t>(bytes);
+            cudaLaunchAttribute at;
+            at.id = cudaLaunchAttributeClusterDimension;
+            at.val.clusterDim.x = nc;
+            at.val.clusterDim.y = 1;
+            at.val.clusterDim.z = 1;
+            cfg.attrs = &at;
+            cfg.numAttrs = 1;
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess || n < 1) {
+                ok = false;
+                break;
+            }
+        }
+        (void)cudaGetLastError();  // a refused size is a plan that does not exist, not an error
+        if (ok) {
+            plan->nc = nc;
+            plan->wmax = wmax;
+            plan->smem = bytes;
+            return true;
+        }
+    }
+    return false;
+}
+
+// `steps` plain steps in one launch of one cluster.
+template <class M>
+cudaError_t do_step_cluster(const LaunchCtx& x, const ClusterPlan& p, void* f0, void* f1, int cur, long long t0,
+                            int steps) {
+    using T = typename M::T;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p.nc);
+    cfg.blockDim = dim3(BX, CLUSTER_THREADS / BX);
+    cfg.dynamicSmemBytes = static_cast<size_t>(p.smem);
+    cfg.stream = x.stream;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = p.nc;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    T* a = static_cast<T*>(f0);
+    T* b = static_cast<T*>(f1);
+    if (x.c.model == 0)
+        return cudaLaunchKernelEx(&cfg, k_step_cluster<M, 0>, x.g, x.ot, x.c, a, b, cur, t0, steps, x.ss.flags, p.wmax);
+    return cudaLaunchKernelEx(&cfg, k_step_cluster<M, 1>, x.g, x.ot, x.c, a, b, cur, t0, steps, x.ss.flags, p.wmax);
 }
 
 template <class M>

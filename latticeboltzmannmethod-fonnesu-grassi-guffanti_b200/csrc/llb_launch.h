@@ -43,6 +43,25 @@ cudaError_t launch_compact_copy_f64(const LaunchCtx&, const CompactGeo&, void*, 
 cudaError_t launch_step_compact_lowp(int storage, const LaunchCtx&, const CompactGeo&, const void*, void*);
 cudaError_t launch_compact_copy_lowp(int storage, const LaunchCtx&, const CompactGeo&, void*, void*, bool);
 
+// Small lattices resident in one thread-block cluster (llb_cluster.cuh):
+// `steps` plain steps from step index t0 in one launch, state f[cur]
+// ping-ponging between f0 and f1.  The host splits longer runs into chunks of
+// CLUSTER_CHUNK steps.
+struct ClusterPlan {
+    int nc = 0;          // blocks of the cluster
+    int wmax = 0;        // columns of the widest slab
+    long long smem = 0;  // dynamic shared memory per block
+};
+constexpr int CLUSTER_CHUNK = 4096;
+bool cluster_plan(int storage, int R, int C, int device, ClusterPlan* plan);
+cudaError_t launch_step_cluster(int storage, const LaunchCtx& ctx, const ClusterPlan& plan, void* f0, void* f1,
+                                int cur, long long t0, int steps);
+bool cluster_plan_f64(int R, int C, int device, ClusterPlan* plan);
+bool cluster_plan_lowp(int storage, int R, int C, int device, ClusterPlan* plan);
+cudaError_t launch_step_cluster_f64(const LaunchCtx&, const ClusterPlan&, void*, void*, int, long long, int);
+cudaError_t launch_step_cluster_lowp(int storage, const LaunchCtx&, const ClusterPlan&, void*, void*, int, long long,
+                                     int);
+
 struct BatchLattice;
 // Batched step over a work list (llb_batch.cuh).  `cooperative` launches the
 // grid cooperatively (required when steps > 1).

@@ -22,6 +22,14 @@ cudaError_t launch_fill_keep_lowp(int storage, const LaunchCtx& x, void* buf) {
 cudaError_t launch_step_compact_lowp(int storage, const LaunchCtx& x, const CompactGeo& cg, const void* fin, void* fout) {
     LLB_DISPATCH((do_step_compact<ModelF32S>(x, cg, fin, fout)), (do_step_compact<ModelF16S>(x, cg, fin, fout)));
 }
+bool cluster_plan_lowp(int storage, int R, int C, int device, ClusterPlan* plan) {
+    LLB_DISPATCH((do_cluster_plan<ModelF32S>(R, C, device, plan)), (do_cluster_plan<ModelF16S>(R, C, device, plan)));
+}
+cudaError_t launch_step_cluster_lowp(int storage, const LaunchCtx& x, const ClusterPlan& p, void* f0, void* f1, int cur,
+                                     long long t0, int steps) {
+    LLB_DISPATCH((do_step_cluster<ModelF32S>(x, p, f0, f1, cur, t0, steps)),
+                 (do_step_cluster<ModelF16S>(x, p, f0, f1, cur, t0, steps)));
+}
 cudaError_t launch_compact_copy_lowp(int storage, const LaunchCtx& x, const CompactGeo& cg, void* dense, void* comp,
                                      bool to_compact) {
     LLB_DISPATCH((do_compact_copy<ModelF32S>(x, cg, dense, comp, to_compact)),

@@ -383,9 +383,11 @@ class CudaLattice:
         return float(ms.value)
 
     def set_pipeline(self, config: int):
-        """-1: one thread per node; -2: the active-sector list; 0..2 and 6: TMA
-        pipeline configurations (6 also loads the tile's bounce bytes); 3..5:
-        two steps per pass through shared memory."""
+        """-1: one thread per node; -2: the active-sector list; -3: compacted
+        planes (active nodes only); -4: the lattice resident in one
+        thread-block cluster's shared memory, a chunk of steps per launch;
+        0..2 and 6: TMA pipeline configurations (6 also loads the tile's
+        bounce bytes); 3..5: two steps per pass through shared memory."""
         _check(lib().llb_set_pipeline(self._h, config), self._h)
 
     @property

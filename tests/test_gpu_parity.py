@@ -91,13 +91,14 @@ def test_f64_bit_exact(case, steps):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
-@pytest.mark.parametrize("pipeline", [-3, -2, 3, 4, 5])
+@pytest.mark.parametrize("pipeline", [-4, -3, -2, 3, 4, 5])
 @pytest.mark.parametrize("steps", [2, 7, 300])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
 def test_f64_list_and_two_step_kernels_bit_exact(case, steps, pipeline):
-    """The compacted-plane kernel (-3), the active-sector list kernel (-2) and
-    the two-steps-per-launch configurations (3-5; odd step counts end with a
-    lone step, 300 steps run through graph replays) on every case."""
+    """The lattice resident in one thread-block cluster (-4), the
+    compacted-plane kernel (-3), the active-sector list kernel (-2) and the
+    two-steps-per-launch configurations (3-5; odd step counts end with a lone
+    step, 300 steps run through graph replays) on every case."""
     name, lists, p, ins, outs = case
     table = H.open_values(lists, ins, outs, steps)
     ref = H.run_oracle(lists, p, steps, table)
@@ -109,11 +110,12 @@ def test_f64_list_and_two_step_kernels_bit_exact(case, steps, pipeline):
     np.testing.assert_array_equal(got["rho"], ref["rho"])
 
 
-@pytest.mark.parametrize("pipeline", [-3, -2, -1, 0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("pipeline", [-4, -3, -2, -1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("case", [CASES[2], CASES[5], CASES[6]], ids=[CASES[2][0], CASES[5][0], CASES[6][0]])
 def test_f64_every_step_kernel_bit_exact(case, pipeline):
-    """The compacted planes (-3), the active-sector list (-2), the
-    one-thread-per-node kernel (-1) and every TMA pipeline configuration."""
+    """The cluster-resident lattice (-4), the compacted planes (-3), the
+    active-sector list (-2), the one-thread-per-node kernel (-1) and every TMA
+    pipeline configuration."""
     name, lists, p, ins, outs = case
     steps = 150
     table = H.open_values(lists, ins, outs, steps)
@@ -153,11 +155,76 @@ def test_cavity129_10k_steps_bit_exact():
     np.testing.assert_array_equal(got["u"], ref["u"])
 
 
+@pytest.mark.parametrize("n,default", [(96, True), (129, False)], ids=["cavity96", "cavity129"])
+@pytest.mark.parametrize("storage", [0, 1, 2], ids=["f64", "f32s", "f16s"])
+def test_cluster_resident_cavity_equals_the_grid(storage, n, default):
+    """A lid cavity resident in one thread-block cluster (-4; the default for
+    96 x 96, chosen explicitly for config 1): runs that cross launch
+    boundaries (4096 steps per launch), odd and even step counts and output
+    steps in between equal the one-thread-per-node kernel bit for bit in
+    every storage form."""
+    lists = H.classify(H.cavity_types(n))
+    p = H.Params(tau=0.884)
+    table = H.open_values(lists, "const:0.1:0", "const:0:0", 1)
+    plan = [(1, False), (4097, False), (3, True), (8192, False), (33, True)]
+    outs = []
+    for pipeline in (None if default else -4, -1):
+        with make_gpu(lists, p, storage=storage, pipeline=pipeline) as g:
+            assert g.pipeline == (-4 if pipeline != -1 else -1)
+            g.set_open_values(table, 0)
+            g.init()
+            for k, macro in plan:
+                g.step(k, macro=macro)
+            outs.append((g.t, g.post_collision(), g.macro()))
+    act = H.active_mask(lists)
+    assert outs[0][0] == outs[1][0] == 1 + sum(k for k, _ in plan)
+    np.testing.assert_array_equal(outs[0][1][:, act], outs[1][1][:, act])
+    np.testing.assert_array_equal(outs[0][2][0], outs[1][2][0])
+    np.testing.assert_array_equal(outs[0][2][1], outs[1][2][1])
+
+
+@pytest.mark.parametrize("storage", [1, 2], ids=["f32s", "f16s"])
+def test_cluster_resident_porous_shifted_equals_every_kernel(storage):
+    """A porous channel whose slabs fit the cluster in the shifted forms
+    (96 x 160, TRT, pressure outlet, uneven slab widths): the cluster-resident
+    lattice gives the bits of every other kernel."""
+    lists = H.classify(H.porous_types(96, 157, fraction=0.25, rmin=2, rmax=5, seed=21))
+    p = H.Params.trt_magic(0.6, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.03:0", "pressure", 1)
+    outs = [run_gpu(lists, p, 203, table, storage=storage, pipeline=cfg) for cfg in (-1, -4, -3, -2, 0, 3, 6)]
+    act = H.active_mask(lists)
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o["post"][:, act], outs[0]["post"][:, act])
+        np.testing.assert_array_equal(o["u"], outs[0]["u"])
+
+
+def test_cluster_resident_refuses_what_does_not_fit():
+    """A lattice whose slabs do not fit one cluster's shared memory refuses
+    pipeline -4 (LLB_E_UNSUPPORTED) and keeps stepping on its kernel."""
+    import llalbm_cuda as L
+
+    lists = H.classify(H.porous_types(300, 400, seed=11))
+    p = H.Params(tau=0.8, outlet_bc=H.BC_ZH_PRESSURE)
+    table = H.open_values(lists, "const:0.02:0", "pressure", 1)
+    with make_gpu(lists, p) as g:
+        before = g.pipeline
+        with pytest.raises(L.LLBError) as e:
+            g.set_pipeline(-4)
+        assert e.value.code == -8 and g.pipeline == before
+        g.set_open_values(pressure_table(table, lists, p), 0)
+        g.init()
+        g.step(20, macro=True)
+        got = g.post_collision()
+    ref = H.run_oracle(lists, p, 21, table)
+    act = H.active_mask(lists)
+    np.testing.assert_array_equal(got[:, act], ref["post"][:, act])
+
+
 def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
-@pytest.mark.parametrize("pipeline", [-3, -2, -1, 0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("pipeline", [-4, -3, -2, -1, 0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3)], ids=["f32s", "f16s"])
 def test_shifted_storage_velocity_error(storage, tol, pipeline):
     lists = H.classify(H.channel_types(64, 160, discs=[(32, 40, 8)]))
@@ -307,14 +374,15 @@ def test_graph_replay_matches_single_launches():
     np.testing.assert_array_equal(outs[0], outs[2])
 
 
-def test_numerics_flag():
+@pytest.mark.parametrize("pipeline", [-4, -1])
+def test_numerics_flag(pipeline):
     """An unstable run (tau near 0.5, strong lid) is reported as LLB_E_NUMERIC."""
     import llalbm_cuda as L
 
     lists = H.classify(H.cavity_types(32))
     p = H.Params(tau=0.5001)
     table = H.open_values(lists, "const:0.6:0", "const:0:0", 1)
-    with make_gpu(lists, p) as g:
+    with make_gpu(lists, p, pipeline=pipeline) as g:
         g.set_open_values(table)
         g.init()
         g.step(5000)
