@@ -71,26 +71,59 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, uns
     return ok_sh != 0;
 }
 
+// Work-list item flag, bit 30 of the item's lattice index: every node of the
+// dense tile is a fluid node whose eight sources are fluid or open (PLAIN; such
+// a node is never on the lattice edge).  The tile then pulls straight from its
+// sources without waiting for its mask bytes: the population loads leave
+// right after the lattice descriptor, one memory round trip earlier.  Set on
+// the host from per-column flags of 32-row segments (k_plain_segments).
+constexpr int ITEM_PLAIN = 1 << 30;
+__host__ __device__ __forceinline__ int item_lattice(int x) { return x & (ITEM_PLAIN - 1); }
+
 // One tile of one lattice: `tile` packs its row-tile index (low 16 bits) and
-// column-tile index (high 16 bits), computed on the host.
+// column-tile index (high 16 bits), computed on the host; plain_tile: the
+// item's ITEM_PLAIN flag.
 template <class M>
-__device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, int tile, long long s) {
+__device__ __forceinline__ void batch_tile(const BatchLattice* __restrict__ Lp, int tile, long long s,
+                                           bool plain_tile) {
     using T = typename M::T;
     const long long d = s - Lp->s0;
+    // both buffers are read with the step fields, so the population addresses
+    // wait for one descriptor round trip, not two
+    const void* const fa = Lp->f[0];
+    const void* const fb = Lp->f[1];
     const int cur = Lp->cur0 ^ static_cast<int>(d & 1);
     const long long t = Lp->t0 + d;
     if (t >= Lp->t_end) return;  // block-uniform: the lattice has finished
-    const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
-    T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
+    const T* __restrict__ fin = static_cast<const T*>(cur ? fb : fa);
+    T* __restrict__ fout = static_cast<T*>(const_cast<void*>(cur ? fa : fb));
     const Geometry& g = Lp->g;  // read where used (L1), not copied into registers
     unsigned* const flags = Lp->flags;
     const int i = (tile & 0xffff) * BX + threadIdx.x;
     const int j = (static_cast<unsigned>(tile) >> 16) * blockDim.y + threadIdx.y;
-    const bool inside = i < g.rows && j < g.cols;
     // 32-bit slot arithmetic: a batch admits only lattices whose nine planes
     // hold fewer than 2^31 slots
     const int P = static_cast<int>(g.plane);
-    const int node = j * g.ld + i;
+    const int ld = g.ld;
+    const int node = j * ld + i;
+    if (plain_tile) {
+        // every lane holds a PLAIN fluid node: the pull of a plain warp, the
+        // moments and the collision, as below
+        typename M::R f[9];
+        f[0] = M::load(fin + node);
+#pragma unroll
+        for (int k = 1; k < 9; ++k) f[k] = M::load(fin + (k * P + node - (DJ(k) * ld + DI(k))));
+        typename M::R rr, xr, yr;
+        M::moments(f, rr, xr, yr);
+        const bool bad = !M::finite(rr);
+        if (Lp->c.model == 0) M::template collide<0>(f, rr, xr, yr, Lp->c);
+        else M::template collide<1>(f, rr, xr, yr, Lp->c);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) M::store(fout + (k * P + node), f[k]);
+        if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
+        return;
+    }
+    const bool inside = i < g.rows && j < g.cols;
     const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
     const uint8_t cls = mask_class(m);
     const bool write_sector = sector_has_active<M>(class_active(cls));
@@ -126,11 +159,13 @@ template <class M>
 __device__ __forceinline__ void batch_slots(const BatchLattice* __restrict__ Lp, int item, long long s) {
     using T = typename M::T;
     const long long d = s - Lp->s0;
+    const void* const fa = Lp->f[0];  // read with the step fields (see batch_tile)
+    const void* const fb = Lp->f[1];
     const long long t = Lp->t0 + d;
     if (t >= Lp->t_end) return;  // block-uniform: the lattice has finished
     const int cur = Lp->cur0 ^ static_cast<int>(d & 1);
-    const T* __restrict__ fin = static_cast<const T*>(Lp->f[cur]);
-    T* __restrict__ fout = static_cast<T*>(Lp->f[cur ^ 1]);
+    const T* __restrict__ fin = static_cast<const T*>(cur ? fb : fa);
+    T* __restrict__ fout = static_cast<T*>(const_cast<void*>(cur ? fa : fb));
     const int nthr = blockDim.x * blockDim.y;
     const long long slot = static_cast<long long>(item) * nthr + threadIdx.y * blockDim.x + threadIdx.x;
     // the descriptor's fields are read where they are used (L1-resident), not
@@ -154,7 +189,7 @@ __global__ void __launch_bounds__(BX* BY, batch_min_blocks<M>()) k_batch_tiles(c
                                                        const int2* __restrict__ items, const long long* sbase,
                                                        long long soff) {
     const int2 it = items[blockIdx.x];
-    batch_tile<M>(lats + it.x, it.y, *sbase + soff);
+    batch_tile<M>(lats + item_lattice(it.x), it.y, *sbase + soff, (it.x & ITEM_PLAIN) != 0);
 }
 
 // ... and the compacted slot blocks, in a launch of their own (each kernel
@@ -182,8 +217,9 @@ __global__ void __launch_bounds__(BX* BY, 5) k_batch_step(const BatchLattice* __
         for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
             const int nxt = item + gridDim.x;
             const int2 it_next = nxt < n_items ? items[nxt] : it;
-            if (lats[it.x].compact) batch_slots<M>(lats + it.x, it.y, s);
-            else batch_tile<M>(lats + it.x, it.y, s);
+            const BatchLattice* Lp = lats + item_lattice(it.x);
+            if (Lp->compact) batch_slots<M>(Lp, it.y, s);
+            else batch_tile<M>(Lp, it.y, s, (it.x & ITEM_PLAIN) != 0);
             it = it_next;
         }
         if (st + 1 < steps && !grid_barrier(bar, bar + 1, gridDim.x, bar_limit)) {
