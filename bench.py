@@ -76,6 +76,18 @@ def workload(name: str, size: int = 4096) -> dict:
     raise SystemExit(f"unknown workload {name}")
 
 
+def workload_config(wl: dict, types: np.ndarray, world: int) -> dict:
+    """The `config` object of a bench line, the same for both arms: the
+    workload, its lattice and its active (fluid, inlet, outlet) node count."""
+    R, C = types.shape
+    n_active = int(np.isin(types, (W.FLUID, W.INLET, W.OUTLET)).sum())
+    return {"workload": wl["name"], "description": wl["desc"], "rows": R, "cols": C, "active_nodes": n_active,
+            "storage": "f64", "pattern": "AB (ping-pong)",
+            "parallelism": f"replicas x{world}" if world > 1 else "one lattice",
+            "l2": "resident state 2 x 9 x 8 B x nodes, far larger than L2: no flush needed"
+            if R * C >= 1 << 20 else "L2-resident lattice"}
+
+
 def open_table(wl: dict, nodes: dict) -> np.ndarray:
     ni, no = len(nodes["inlet"]), len(nodes["outlet"])
     tab = np.zeros((1, ni + no, 2))
@@ -525,11 +537,7 @@ def run_ours(a, dist):
         "metric": METRIC, "value": round(f64["mlups"], 1), "unit": "MLUPS", "n_gpus": dist.world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(f64["ms_per_step"], 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl["name"], "description": wl["desc"], "rows": R, "cols": C,
-                   "active_nodes": n_active, "storage": "f64", "pattern": "AB (ping-pong)",
-                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
-                   "l2": "resident state 2 x 9 x 8 B x nodes, far larger than L2: no flush needed"
-                   if R * C >= 1 << 20 else "L2-resident lattice"},
+        "config": workload_config(wl, types, dist.world),
         "roofline": {"bound": "hbm", "achieved": round(f64["gb_s"], 1), "peak": peak, "unit": "GB/s",
                      "frac": round(f64["gb_s"] / peak, 4), "traffic": traffic,
                      "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
@@ -918,7 +926,7 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return
-        w = min(a.warmup, 2)
+        w = min(a.warmup, 5)
         if a.workload in ("batch256", "serve"):
             # a sample of the independent problems, each through its own Lattice
             if a.workload == "batch256":
@@ -933,14 +941,20 @@ def main():
                 desc = "served request stream (sample of 6 requests)"
             k = max(1, min(a.steps, 20))
             r = reference_sample(items, w, k)
-            wl = {"name": a.workload, "desc": desc}
+            wl = {"name": a.workload, "desc": desc, "config": {"workload": a.workload, "description": desc}}
             if r is None:
                 print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_runner_fast was not built"}))
                 return
         else:
             wl = workload(a.workload, a.size)
             types = wl["types"]()
-            k = max(1, min(a.steps, 5 if a.workload == "porous4096" else 200))
+            # K timed steps of the whole lattice after W warm-up steps, as the
+            # GPU arm, as long as they stay within about 40 steps of the 4096^2
+            # lattice (~2 minutes on 16 host threads); beyond that, fewer
+            # steps, reported as such
+            cap = max(2, 40 * 4096 * 4096 // (types.shape[0] * types.shape[1]))
+            w = min(a.warmup, max(1, cap // 8))
+            k = max(1, min(a.steps, cap - w))
             r = reference_cpu(wl, types, w, k)
             if r is None:
                 r = oracle_cpu(wl, types, k)
@@ -951,7 +965,7 @@ def main():
             "impl": "reference", "metric": METRIC, "value": round(r["value"], 3), "unit": "MLUPS",
             "n_gpus": 0, "steps": k, "warmup": w, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wl["name"], "description": wl["desc"]},
+            "config": wl["config"] if "config" in wl else workload_config(wl, types, 1),
             "cpu_baseline": r, "e2e": {"value": round(r["value"], 3), "unit": "MLUPS",
                                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }), flush=True)
