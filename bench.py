@@ -820,7 +820,7 @@ def run_serve(a, dist):
             b.add(r["rows"], r["cols"], n["fluid"], n["wall"], n["inlet"], n["inlet_side"], n["outlet"],
                   n["outlet_side"], n["obstacle"], n["obstacle_dirs"], collision=r["collision"], tau=r["tau"],
                   tau_even=r["tau_even"], tau_odd=r["tau_odd"], outlet_bc=r["outlet_bc"], open_values=p["table"])
-        b.set_layout(L.LAYOUT_COMPACT)   # the server's lanes' layout and shape
+        b.set_layout(L.LAYOUT_AUTO)      # the server's lanes' layout and shape
         b.set_config(2, 1)
         b.step(32)
         b.synchronize()

@@ -26,25 +26,7 @@ using namespace llb;
 
 namespace {
 constexpr int BATCH_GRAPH_STEPS = 32;  // even: a replay keeps every lattice's buffer parity
-
-// 1 per (32-row segment ti, column j) of a dense lattice, out[j * nti + ti],
-// when all 32 rows of the segment exist and are PLAIN fluid nodes.  One warp
-// per segment.
-__global__ void __launch_bounds__(256) k_plain_segments(const uint8_t* __restrict__ mask, int rows, int cols, int ld,
-                                                        int nti, uint8_t* __restrict__ out) {
-    const long long w = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= static_cast<long long>(nti) * cols) return;  // warp-uniform
-    const int j = static_cast<int>(w / nti);
-    const int i = static_cast<int>(w - static_cast<long long>(j) * nti) * BX + lane;
-    bool ok = i < rows;
-    if (ok) {
-        const uint8_t m = mask[static_cast<long long>(j) * ld + i];
-        ok = mask_class(m) == CLS_FLUID && (m & MASK_PLAIN);
-    }
-    ok = __all_sync(0xffffffffu, ok);
-    if (lane == 0) out[w] = ok ? 1 : 0;
-}
+static_assert(BX == 32, "a handle's plain_seg flags segments of 32 rows, one dense tile's rows");
 }  // namespace
 
 struct llb_batch {
@@ -54,9 +36,6 @@ struct llb_batch {
     int sm_count = 148;
     std::vector<llb_handle> slot;        // nullptr: free slot
     std::vector<BatchLattice> desc;      // per slot
-    // per slot: k_plain_segments of the lattice (32-row segments of each
-    // column that hold only PLAIN fluid nodes), for the items' ITEM_PLAIN flags
-    std::vector<std::vector<uint8_t>> plain_seg;
     std::vector<int> order;              // active slots in descriptor order
     BatchLattice* d_desc = nullptr;
     int desc_cap = 0;
@@ -179,7 +158,7 @@ int rebuild(llb_batch_handle b) {
             // tiles in column-major order, (row tile, column tile) packed in 16
             // bits each; ITEM_PLAIN on tiles whose every node is a PLAIN fluid node
             const int by = b->block_y, cols = d.g.cols, ntj = (cols + by - 1) / by;
-            const std::vector<uint8_t>& seg = b->plain_seg[s];
+            const std::vector<uint8_t>& seg = b->slot[s]->plain_seg;
             const bool have = seg.size() == static_cast<size_t>(d.nti) * static_cast<size_t>(cols);
             for (int tj = 0; tj < ntj; ++tj)
                 for (int ti = 0; ti < d.nti; ++ti) {
@@ -384,25 +363,6 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
     // lattices without them run on the dense ones
     const bool compact = want_compact(b, h);
     if (!compact && handle_leave_compact(h) != LLB_OK) return bfail(b, LLB_E_CUDA, llb_last_error(h));
-    // the lattice's 32-row column segments that hold only PLAIN fluid nodes
-    // (its mask does not change), computed on its own stream
-    std::vector<uint8_t> seg;
-    {
-        const LaunchCtx x0 = handle_ctx(h);
-        const int nti = static_cast<int>((h->R + BX - 1) / BX);
-        const size_t n = static_cast<size_t>(nti) * static_cast<size_t>(h->C);
-        uint8_t* d_seg = nullptr;
-        seg.resize(n);
-        LLB_BCUDA(b, cudaMallocAsync(reinterpret_cast<void**>(&d_seg), n, h->stream));
-        const long long threads = static_cast<long long>(n) * 32;
-        k_plain_segments<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, h->stream>>>(
-            x0.g.mask, static_cast<int>(h->R), static_cast<int>(h->C), x0.g.ld, nti, d_seg);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(seg.data(), d_seg, n, cudaMemcpyDeviceToHost, h->stream);
-        const cudaError_t ef = cudaFreeAsync(d_seg, h->stream);
-        if (e == cudaSuccess) e = ef;
-        if (e != cudaSuccess) return bfail(b, LLB_E_CUDA, std::string("plain segments: ") + cudaGetErrorString(e));
-    }
     // the lattice works on the batch's stream from now on
     LLB_BCUDA(b, cudaStreamSynchronize(h->stream));
     cudaStreamDestroy(h->stream);
@@ -439,11 +399,9 @@ int llb_batch_attach(llb_batch_handle b, llb_handle h, int32_t* slot) {
     if (s == static_cast<int>(b->slot.size())) {
         b->slot.push_back(nullptr);
         b->desc.push_back(BatchLattice{});
-        b->plain_seg.emplace_back();
     }
     b->slot[s] = h;
     b->desc[s] = d;
-    b->plain_seg[s] = std::move(seg);
     b->dirty = true;
     *slot = s;
     return LLB_OK;
@@ -469,7 +427,6 @@ int llb_batch_detach(llb_batch_handle b, int32_t slot, llb_handle* out) {
     h->stream = st;
     h->own_stream = true;
     b->slot[slot] = nullptr;
-    b->plain_seg[slot].clear();
     b->dirty = true;
     *out = h;
     return LLB_OK;

@@ -76,7 +76,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, uns
 // a node is never on the lattice edge).  The tile then pulls straight from its
 // sources without waiting for its mask bytes: the population loads leave
 // right after the lattice descriptor, one memory round trip earlier.  Set on
-// the host from per-column flags of 32-row segments (k_plain_segments).
+// the host from the lattice's per-column flags of 32-row segments (built with
+// its mask).
 constexpr int ITEM_PLAIN = 1 << 30;
 __host__ __device__ __forceinline__ int item_lattice(int x) { return x & (ITEM_PLAIN - 1); }
 

@@ -777,6 +777,20 @@ int llb_create(const llb_desc* d, llb_handle* out) {
     int rc = build_mask(d, h->ld, mask, bb, ps, psb, open_idx, h->n_nonplain, why);
     if (rc != LLB_OK) { delete h; return fail(nullptr, rc, why); }
     h->n_active = d->n_fluid + d->n_inlet + d->n_outlet;
+    {
+        constexpr int64_t SEG = 32;  // rows of a warp of the batch's dense tiles
+        const int64_t nti = (h->R + SEG - 1) / SEG;
+        h->plain_seg.assign(static_cast<size_t>(nti * h->C), 0);
+        for (int64_t j = 0; j < h->C; ++j)
+            for (int64_t ti = 0; ti < nti; ++ti) {
+                bool ok = (ti + 1) * SEG <= h->R;
+                for (int64_t i = ti * SEG; ok && i < (ti + 1) * SEG; ++i) {
+                    const uint8_t m = mask[static_cast<size_t>(j * h->ld + i)];
+                    ok = mask_class(m) == CLS_FLUID && (m & MASK_PLAIN);
+                }
+                h->plain_seg[static_cast<size_t>(j * nti + ti)] = ok ? 1 : 0;
+            }
+    }
     h->tma_cfg = default_pipeline(*h);
     if (!ps.empty()) h->tma_cfg = -1;  // partially saturated obstacles: one thread per node only
     int ndev = 0;

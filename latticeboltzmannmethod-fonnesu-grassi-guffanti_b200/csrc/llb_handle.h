@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/llalbm_cuda.h"
 #include "llb_launch.h"
@@ -89,6 +90,10 @@ struct llb_lattice {
     int where = 0;
     // polls of the pipelined kernels' stage waits before they give up
     long long wait_limit = llb::DEFAULT_WAIT_LIMIT;
+    // per (32-row segment ti, column j), plain_seg[j * ceil(R / 32) + ti]: 1
+    // when all 32 rows of the segment exist and are PLAIN fluid nodes (built
+    // with the mask; a batch flags its all-PLAIN dense tiles from it)
+    std::vector<uint8_t> plain_seg;
     // the lattice resident in one thread-block cluster (pipeline
     // PIPE_CLUSTER): its plan, looked up once (cl_state 0 not yet, 1 it
     // fits, -1 it does not)
