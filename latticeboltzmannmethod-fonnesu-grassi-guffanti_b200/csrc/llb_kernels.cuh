@@ -45,7 +45,7 @@ __device__ __forceinline__ void pull(const Geometry& g, const typename M::T* __r
 #pragma unroll
         for (int k = 1; k < 9; ++k) f[k] = M::load(fin + (k * P + node - (DJ(k) * ld + DI(k))));
     } else if (i > 0 && j > 0 && i < g.rows - 1 && j < g.cols - 1) {
-        const unsigned b = (m & MASK_PLAIN) ? 0u : (b_pre != NO_BB ? b_pre : g.bb[node]);
+        const unsigned b = (m & MASK_PLAIN) ? 0u : (b_pre != NO_BB ? b_pre : ld_keep(g.bb + node, l2_keep_policy()));
 #pragma unroll
         for (int k = 1; k < 9; ++k) {
             const I a = ((b >> (k - 1)) & 1u) ? opp(k) * P + node : k * P + node - (DJ(k) * ld + DI(k));
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(BX* BY) k_step(Geometry g, OpenTable ot, Colli
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const bool inside = i < g.rows && j < g.cols;
     const long long node = static_cast<long long>(j) * g.ld + i;
-    const uint8_t m = inside ? g.mask[node] : CLS_DEAD;
+    const uint8_t m = inside ? ld_keep(g.mask + node, l2_keep_policy()) : CLS_DEAD;
     const bool write_sector = sector_has_active<M>(class_active(mask_class(m)));
     pdl_wait_then_release();
     step_node<M, COLL, MACRO, INIT, PS>(g, ot, c, fin, fout, mo, ss, i, j, node, inside, m, write_sector,
