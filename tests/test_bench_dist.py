@@ -43,3 +43,28 @@ def test_replica_timing_is_the_max_over_ranks():
         p.join(timeout=30)
         assert p.exitcode == 0
     assert res == {0: 3.0, 1: 3.0}
+
+
+@pytest.mark.timeout(300)
+def test_reference_arm_reports_the_gpu_arms_config_and_steps():
+    """The reference arm (LLALBM's own OpenMP perform_lbm on the host cores)
+    prints one JSON line on the GPU arm's config object, with the K timed
+    steps and W warm-up steps it was asked for."""
+    import json
+    import subprocess
+
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_runner_fast")):
+        pytest.skip("the reference runner is not built (oracle/Makefile)")
+    sys.path.insert(0, ROOT)
+    import bench
+
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                        "cavity129", "--steps", "7", "--warmup", "4"], capture_output=True, text=True, timeout=240,
+                       cwd=ROOT)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["unit"] == "MLUPS" and line["value"] > 0
+    assert (line["steps"], line["warmup"]) == (7, 4)
+    wl = bench.workload("cavity129")
+    assert line["config"] == bench.workload_config(wl, wl["types"](), 1)
+    assert line["e2e"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "reference"
